@@ -1,0 +1,219 @@
+/*
+ * csffci_b200.h -- C ABI of the B200 CSF-basis FCI engine (libcsffci_b200.so).
+ *
+ * Every function takes DEVICE pointers (caller-owned buffers, e.g. from
+ * torch), explicit sizes and a cudaStream_t, launches asynchronously on that
+ * stream and returns CSFFCI_OK or a negative status; the text of the last
+ * error on the calling host thread is returned by csffci_last_error().
+ * Functions are re-entrant across streams as long as their output and
+ * workspace buffers are distinct.  Nothing allocates device memory except
+ * where a function says so; workspaces are passed in.
+ *
+ * Layouts (all row-major):
+ *   determinant CI vector  f64[Na][Nb]      alpha-major, strings in ascending
+ *                                           integer (colex) order
+ *   CSF CI vector          f64[ncsf]        npair -> doubly-occupied config ->
+ *                                           singly-occupied config -> genealogical
+ *                                           coupling (pyscf/csf_fci/csdstring.py:10-14,
+ *                                           pyscf/csf_fci/csfstring.py:806-849)
+ *   two-electron integrals f64[npair][npair] four-fold pair matrix, pair index
+ *                                           hi*(hi+1)/2+lo (pyscf/lib/mcscf/fci_gas.h:171-176)
+ *   link table             csffci_link_t[N][nlink], row order of
+ *                                           pyscf/lib/mcscf/fci_string_gas.c:1341-1382
+ */
+#ifndef CSFFCI_B200_H
+#define CSFFCI_B200_H
+
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  CSFFCI_OK = 0,
+  CSFFCI_ERR_INVALID = -1, /* bad argument (same meaning as GAS_ERR_INVALID, fci_gas.h:38-42) */
+  CSFFCI_ERR_MEMORY = -2,  /* workspace too small (GAS_ERR_MEMORY) */
+  CSFFCI_ERR_CUDA = -3,    /* a CUDA runtime call failed */
+  CSFFCI_ERR_TIMEOUT = -4  /* a bounded device-side wait gave up */
+};
+
+/* One spin-string excitation a+_cre a_des |I> = sign |addr>; byte layout of
+ * gas_link_entry_t in raw format (pyscf/lib/mcscf/fci_gas.h:94-105):
+ * op = cre | des << 8. */
+typedef struct {
+  uint32_t addr;
+  uint16_t op;
+  int8_t sign;
+  uint8_t pad;
+} csffci_link_t;
+
+/* One npair block of the CSF <-> determinant map (the loop body of
+ * _transform_det2csf, pyscf/csf_fci/csfstring.py:596-659). umat is a device
+ * pointer to f64[ndet][ncsf] (the spin eigenvectors of the block, without
+ * the block sign). */
+typedef struct {
+  int64_t csd_offset;  /* first CSD (and det) index of the block            */
+  int64_t csf_offset;  /* first CSF index of the block                      */
+  int64_t nconf;       /* configurations in the block                       */
+  int32_t ndet;        /* spin determinants per configuration               */
+  int32_t ncsf;        /* CSFs per configuration (0: block dropped)         */
+  int32_t nspin;       /* unpaired electrons                                */
+  int32_t npair;       /* doubly occupied orbitals                          */
+  double sign;         /* (-1)^ncomm, csfstring.py:623-627                  */
+  const double* umat;  /* device f64[ndet][ncsf]                            */
+  const double* zmat;  /* device f64[nspin*(nspin-1)/2][ncsf] exchange
+                          expectation table for hdiag_csf (may be NULL for
+                          transforms)                                        */
+} csffci_block_t;
+
+int csffci_abi_version(void);
+const char* csffci_last_error(void);
+
+/* ---- strings and link tables (PySCF cistring; reference twin
+ *      pyscf/lib/mcscf/fci_string_gas.c:263-298, 1304-1427) ------------- */
+
+/* strs[i] = i-th occupation string of nelec electrons in norb orbitals. */
+int csffci_gen_strings(int norb, int nelec, uint64_t* strs, cudaStream_t stream);
+
+/* link[I][k], nlink = nelec*(norb-nelec+1); bit-exact with the raw
+ * fill_link_table of fci_string_gas.c:1304-1427. */
+int csffci_link_table(int norb, int nelec, csffci_link_t* link, cudaStream_t stream);
+
+/* ---- CSD / configuration masks (csdstring.py:28-65, csfstring.py:789-804,
+ *      csfstring.c:13-83) ----------------------------------------------- */
+
+/* csd_mask[idx_csd] = idx_det; econf_det_mask[idx_det] = configuration;
+ * econf_csf_mask[idx_csf] = configuration (any output may be NULL). */
+int csffci_csd_masks(int norb, int neleca, int nelecb, int smult,
+                     uint32_t* csd_mask, uint32_t* econf_det_mask,
+                     uint32_t* econf_csf_mask, cudaStream_t stream);
+
+/* ---- genealogical spin couplings (csfstring.py:806-960, csfstring.c:86-293) */
+
+/* umat[det][csf] for nspin unpaired electrons, 2MS = neleca-nelecb, 2S+1 =
+ * smult; bit-exact with FCICSFmakecsf (csfstring.c:86-141). */
+int csffci_spin_evecs(int nspin, int neleca, int nelecb, int smult, double* umat,
+                      cudaStream_t stream);
+
+/* zmat[(a,b)][csf] = sum_x umat[x][csf] umat[swap_ab(x)][csf] (-1)^(b-a-1):
+ * the expectation value, per CSF, of the signed spin exchange of unpaired
+ * positions a<b; used by csffci_hdiag_csf in place of the per-configuration
+ * blocks built by FCICSFhdiag (csfstring.c:295-362). */
+int csffci_spin_exchange_table(int nspin, int neleca, int nelecb, int smult,
+                               const double* umat, double* zmat, cudaStream_t stream);
+
+/* ---- det <-> CSF transforms, batched over nvec vectors
+ *      (transform_civec_det2csf / _csf2det, csfstring.py:341-487,569-674) */
+int csffci_det2csf(int nvec, const double* x_det, int64_t ld_det, double* x_csf,
+                   int64_t ld_csf, const uint32_t* csd_mask,
+                   const csffci_block_t* blocks, int nblock, cudaStream_t stream);
+/* x_det is fully overwritten (determinants of dropped blocks are zero). */
+int csffci_csf2det(int nvec, const double* x_csf, int64_t ld_csf, double* x_det,
+                   int64_t ld_det, int64_t ndet, const uint32_t* csd_mask,
+                   const csffci_block_t* blocks, int nblock, cudaStream_t stream);
+
+/* ---- Hamiltonian pieces ------------------------------------------------ */
+
+/* h2e[pq][rs] = fac*(eri[pq][rs] + delta_{p=q} f[r,s] + delta_{r=s} f[p,q]),
+ * f = (h1e - 1/2 sum_k (pk|kq)) / nelec.  Replaces direct_spin1.absorb_h1e
+ * called at csf.py:445,520. */
+int csffci_absorb_h1e(int norb, int nelec, const double* h1e, const double* eri,
+                      double fac, double* h2e, cudaStream_t stream);
+
+/* Determinant diagonal with (alpha, beta) one-electron parts; replaces
+ * direct_uhf.make_hdiag at csf.py:66-68 (reference twin
+ * fci_hdiag_gas.c:678-709).  work: >= csffci_hdiag_det_workspace() bytes. */
+size_t csffci_hdiag_det_workspace(int norb, int neleca, int nelecb);
+int csffci_hdiag_det(int norb, int neleca, int nelecb, const double* h1a,
+                     const double* h1b, const double* eri, double* hdiag,
+                     void* work, size_t work_bytes, cudaStream_t stream);
+
+/* CSF diagonal computed per configuration on the fly (make_hdiag_csf,
+ * csf.py:70-144, which materialises (nconf,ndet,ndet) blocks instead).
+ * blocks[i].zmat must be set (csffci_spin_exchange_table). */
+int csffci_hdiag_csf(int norb, int neleca, int nelecb, const double* hdiag_det,
+                     const double* eri, const uint32_t* csd_mask,
+                     const csffci_block_t* blocks, int nblock, double* hdiag_csf,
+                     cudaStream_t stream);
+
+/* Slater-Condon H among n determinants (full symmetric matrix, diagonal
+ * from hdiag_det); replaces libfci.FCIpspace_h0tril_uhf + hermi_triu at
+ * csf.py:313-326. */
+int csffci_pspace_h0(int norb, int neleca, int nelecb, const double* h1a,
+                     const double* h1b, const double* eri, const double* hdiag_det,
+                     const uint32_t* det_addr, int n, double* h0, cudaStream_t stream);
+
+/* ---- sigma (direct_spin1.contract_2e at csf.py:449,525-529; reference twin
+ *      fci_contract_gas_plan_execute, fci_contract_gas.c:2423-2452) ------- */
+
+enum {
+  CSFFCI_SIGMA_ACCUMULATE = 1, /* add into sigma instead of overwriting */
+  CSFFCI_SIGMA_SPIN_SYMMETRIC = 2 /* ci == eta * ci^T (na == nb): only the
+                                     row-local half is formed, then
+                                     sigma = s + eta * s^T */
+};
+
+size_t csffci_sigma_workspace(int norb, int neleca, int nelecb, int flags);
+/* sigma = sum_{pq,rs} h2e[pq][rs] E_pq E_rs ci.  eta (+1/-1) is used only
+ * with CSFFCI_SIGMA_SPIN_SYMMETRIC. */
+int csffci_sigma(int norb, int neleca, int nelecb, const double* h2e,
+                 const csffci_link_t* link_a, const csffci_link_t* link_b,
+                 const double* ci, double* sigma, int flags, int eta, void* work,
+                 size_t work_bytes, cudaStream_t stream);
+
+/* sigma += sum_pq h1a[p,q] Ea_pq ci + h1b[p,q] Eb_pq ci (direct_uhf.contract_1e
+ * as used for the spin part of h1e at csf.py:527-528). */
+int csffci_contract_1e(int norb, int neleca, int nelecb, const double* h1a,
+                       const double* h1b, const csffci_link_t* link_a,
+                       const csffci_link_t* link_b, const double* ci, double* sigma,
+                       cudaStream_t stream);
+
+/* ---- density matrices (direct_spin1.make_rdm12/trans_rdm12, inherited at
+ *      csf.py:557; reference twin fci_rdm_gas_plan_make_rdm12s,
+ *      fci_rdm_gas.c:2207-2243, assembled as fci_gas.py:724-733) --------- */
+
+size_t csffci_rdm12_workspace(int norb, int neleca, int nelecb);
+/* dm1[p][q] = <bra|q+ p|ket>, dm2[p][q][r][s] = <bra|p+ r+ s q|ket>
+ * (fci_gas.h:260-268).  dm2 may be NULL (1-RDM only). */
+int csffci_rdm12(int norb, int neleca, int nelecb, const csffci_link_t* link_a,
+                 const csffci_link_t* link_b, const double* bra, const double* ket,
+                 double* dm1, double* dm2, void* work, size_t work_bytes,
+                 cudaStream_t stream);
+
+/* ---- Davidson update (role of pyscf lib.davidson1 via fci.eig at
+ *      csf.py:487-490) --------------------------------------------------- */
+
+/* out[i][j] = sum_k x[i][k] y[j][k]  (nx x ny Gram block, vectors of
+ * length n with leading dimensions ldx, ldy); split over the length with a
+ * fixed-order final reduction (bit-reproducible). */
+size_t csffci_gram_workspace(int nx, int ny, int64_t n);
+int csffci_gram(int nx, const double* x, int64_t ldx, int ny, const double* y,
+                int64_t ldy, int64_t n, double* out, void* work, size_t work_bytes,
+                cudaStream_t stream);
+/* y[r][:] = beta*y[r][:] + sum_i coef[r][i] x[i][:], r < ny, i < nx
+ * (coef is a device f64[ny][nx]). */
+int csffci_combine(int ny, double* y, int64_t ldy, double beta, int nx,
+                   const double* x, int64_t ldx, const double* coef, int64_t n,
+                   cudaStream_t stream);
+/* Davidson/Olsen correction vector for one root (Davidson-Liu with
+ * Olsen's correction, J. Olsen, P. Jorgensen, J. Simons, CPL 169, 463
+ * (1990); the reference obtains it from fci.make_precond, csf.py:433):
+ *   t = (r - e1 x) * P,  P = 1/(hdiag - (e - shift)) with |P| capped at 1e8
+ * mode 0: e1 = 0;  mode 1: e1 = (x.P r)/(x.P x) over the diagonal P;
+ * mode 2: e1 given (the caller folds an exact p-space block into it).
+ * work: csffci_precond_workspace() bytes. */
+size_t csffci_precond_workspace(void);
+int csffci_precond(int64_t n, const double* r, const double* x, const double* hdiag,
+                   double e, double shift, int mode, double e1, double* t, double* work,
+                   cudaStream_t stream);
+/* out2[0] = x.(P r), out2[1] = x.(P x) over the diagonal P (device). */
+int csffci_precond_dots(int64_t n, const double* r, const double* x, const double* hdiag,
+                        double e, double shift, double* out2, double* work,
+                        cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CSFFCI_B200_H */

@@ -1,0 +1,122 @@
+"""ctypes binding of libcsffci_b200.so (declared in include/csffci_b200.h).
+
+The library is the only compute path: if it cannot be loaded, every entry
+point of this package raises.  There is no CPU fallback.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcsffci_b200.so")
+
+CSFFCI_OK = 0
+CSFFCI_ERR_INVALID = -1
+CSFFCI_ERR_MEMORY = -2
+CSFFCI_ERR_CUDA = -3
+CSFFCI_ERR_TIMEOUT = -4
+
+SIGMA_ACCUMULATE = 1
+SIGMA_SPIN_SYMMETRIC = 2
+
+
+class LinkEntry(ctypes.Structure):
+    """csffci_link_t: byte layout of the raw gas_link_entry_t
+    (pyscf/lib/mcscf/fci_gas.h:94-105)."""
+    _fields_ = [("addr", ctypes.c_uint32), ("op", ctypes.c_uint16),
+                ("sign", ctypes.c_int8), ("pad", ctypes.c_uint8)]
+
+
+class Block(ctypes.Structure):
+    """csffci_block_t: one npair block of the CSF <-> determinant map."""
+    _fields_ = [("csd_offset", ctypes.c_int64), ("csf_offset", ctypes.c_int64),
+                ("nconf", ctypes.c_int64), ("ndet", ctypes.c_int32), ("ncsf", ctypes.c_int32),
+                ("nspin", ctypes.c_int32), ("npair", ctypes.c_int32), ("sign", ctypes.c_double),
+                ("umat", ctypes.c_void_p), ("zmat", ctypes.c_void_p)]
+
+
+assert ctypes.sizeof(LinkEntry) == 8
+assert ctypes.sizeof(Block) == 64
+
+_i = ctypes.c_int
+_i64 = ctypes.c_int64
+_sz = ctypes.c_size_t
+_d = ctypes.c_double
+_p = ctypes.c_void_p
+
+_SIGS = {
+    "csffci_abi_version": ([], _i),
+    "csffci_last_error": ([], ctypes.c_char_p),
+    "csffci_gen_strings": ([_i, _i, _p, _p], _i),
+    "csffci_link_table": ([_i, _i, _p, _p], _i),
+    "csffci_csd_masks": ([_i, _i, _i, _i, _p, _p, _p, _p], _i),
+    "csffci_spin_evecs": ([_i, _i, _i, _i, _p, _p], _i),
+    "csffci_spin_exchange_table": ([_i, _i, _i, _i, _p, _p, _p], _i),
+    "csffci_det2csf": ([_i, _p, _i64, _p, _i64, _p, _p, _i, _p], _i),
+    "csffci_csf2det": ([_i, _p, _i64, _p, _i64, _i64, _p, _p, _i, _p], _i),
+    "csffci_absorb_h1e": ([_i, _i, _p, _p, _d, _p, _p], _i),
+    "csffci_hdiag_det_workspace": ([_i, _i, _i], _sz),
+    "csffci_hdiag_det": ([_i, _i, _i, _p, _p, _p, _p, _p, _sz, _p], _i),
+    "csffci_hdiag_csf": ([_i, _i, _i, _p, _p, _p, _p, _i, _p, _p], _i),
+    "csffci_pspace_h0": ([_i, _i, _i, _p, _p, _p, _p, _p, _i, _p, _p], _i),
+    "csffci_sigma_workspace": ([_i, _i, _i, _i], _sz),
+    "csffci_sigma": ([_i, _i, _i, _p, _p, _p, _p, _p, _i, _i, _p, _sz, _p], _i),
+    "csffci_contract_1e": ([_i, _i, _i, _p, _p, _p, _p, _p, _p, _p], _i),
+    "csffci_rdm12_workspace": ([_i, _i, _i], _sz),
+    "csffci_rdm12": ([_i, _i, _i, _p, _p, _p, _p, _p, _p, _p, _sz, _p], _i),
+    "csffci_gram_workspace": ([_i, _i, _i64], _sz),
+    "csffci_gram": ([_i, _p, _i64, _i, _p, _i64, _i64, _p, _p, _sz, _p], _i),
+    "csffci_combine": ([_i, _p, _i64, _d, _i, _p, _i64, _p, _i64, _p], _i),
+    "csffci_precond_workspace": ([], _sz),
+    "csffci_precond": ([_i64, _p, _p, _p, _d, _d, _i, _d, _p, _p, _p], _i),
+    "csffci_precond_dots": ([_i64, _p, _p, _p, _d, _d, _p, _p, _p], _i),
+}
+
+_LIB = None
+
+
+class CSFFCIError(RuntimeError):
+    def __init__(self, name, status, message):
+        super().__init__("%s failed (status %d): %s" % (name, status, message))
+        self.status = status
+
+
+def exported_symbols():
+    return sorted(_SIGS)
+
+
+def load():
+    """Load (building first if the sources are newer and nvcc exists)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    try:
+        from . import build as _build
+        if not _build.up_to_date():
+            _build.build()
+    except Exception:  # no nvcc on this machine: use the shipped library
+        pass
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libcsffci_b200.so is missing (%s); build it with "
+                          "python pyscf-forge_b200/build.py" % LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (args, res) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _LIB = lib
+    return lib
+
+
+def call(name, *args):
+    lib = load()
+    st = getattr(lib, name)(*args)
+    if st != CSFFCI_OK:
+        msg = lib.csffci_last_error().decode(errors="replace")
+        if st == CSFFCI_ERR_MEMORY:
+            raise MemoryError("%s: %s" % (name, msg))
+        raise CSFFCIError(name, st, msg)
+    return st
+
+
+def query(name, *args):
+    return getattr(load(), name)(*args)

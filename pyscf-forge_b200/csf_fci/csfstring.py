@@ -1,0 +1,440 @@
+"""CSFTransformer on the GPU: genealogical CSF addressing, spin eigenvectors
+and the CSF <-> determinant transforms.
+
+Mirrors pyscf/csf_fci/csfstring.py (class CSFTransformer 33-223 and the
+module functions it uses).  The masks (csd_mask, econf_det_mask,
+econf_csf_mask) and the per-npair spin eigenvector blocks live on the device
+and are built once per (norb, neleca, nelecb, smult), as in
+_update_spin_cache (csfstring.py:105-115); unlike the reference the spin
+eigenvectors are cached instead of being rebuilt on every transform
+(csfstring.py:630).
+"""
+import ctypes
+from math import comb
+
+import numpy as np
+import torch
+
+from .. import _capi
+from .._runtime import device, ptr, require_cuda, stream, to_dev, workspace
+from .csdstring import get_csdaddrs_shape, check_csd_mask_size
+
+
+class ImpossibleCIvecError(RuntimeError):
+    """csfstring.py:15-25."""
+
+    def __init__(self, message, ndet=None, ncsf=None, norb=None, neleca=None, nelecb=None):
+        self.message = message
+        self.ndet = ndet
+        self.ncsf = ncsf
+        self.norb = norb
+        self.neleca = neleca
+        self.nelecb = nelecb
+
+    def __str__(self):
+        return self.message
+
+
+class ImpossibleSpinError(ImpossibleCIvecError):
+    """csfstring.py:27-31."""
+
+    def __init__(self, message, ndet=None, ncsf=None, norb=None, neleca=None, nelecb=None, smult=None):
+        ImpossibleCIvecError.__init__(self, message, ndet=ndet, ncsf=ncsf, norb=norb,
+                                      neleca=neleca, nelecb=nelecb)
+        self.smult = smult
+
+
+def csf_gentable(nspin, smult):
+    """Genealogical path-count table (csfstring.py:806-849)."""
+    assert (smult - 1) % 2 == nspin % 2, "{} {}".format(smult, nspin)
+    if smult > nspin + 1:
+        return np.zeros((1, 1), dtype=np.int32)
+    n0 = (nspin - (smult - 1)) // 2
+    n1 = (nspin + (smult - 1)) // 2
+    g = np.zeros((n0 + 1, n1 + 1), dtype=np.int64)
+    g[n0, n0:] = 1
+    for i0 in range(n0, 0, -1):
+        row = list(g[i0, i0:])
+        row = [sum(row[i1:]) for i1 in range(len(row))]
+        row = [row[0]] + row
+        g[i0 - 1, i0 - 1:] = row
+    return g.astype(np.int32)
+
+
+def count_csfs(nspin, smult):
+    """csfstring.py:851-852 (closed form of the table's corner)."""
+    twoS = smult - 1
+    if twoS > nspin or (nspin - twoS) % 2:
+        return 0
+    n0 = (nspin - twoS) // 2
+    return comb(nspin, n0) - (comb(nspin, n0 - 1) if n0 > 0 else 0)
+
+
+def get_csfvec_shape(norb, neleca, nelecb, smult):
+    """csfstring.py:858-911: (min_npair, npair_offset, npair_dconf_size,
+    npair_sconf_size, npair_csf_size)."""
+    s = (smult - 1) / 2
+    ms = (neleca - nelecb) / 2
+    nless = min(neleca, nelecb)
+    if neleca > norb or nelecb > norb or neleca < 0 or nelecb < 0:
+        raise ImpossibleCIvecError("({}e+{}e,{}o)".format(neleca, nelecb, norb),
+                                   norb=norb, neleca=neleca, nelecb=nelecb)
+    if abs(neleca - nelecb) > smult - 1:
+        raise ImpossibleSpinError("Impossible quantum numbers: s = {}; ms = {}".format(s, ms),
+                                  norb=norb, neleca=neleca, nelecb=nelecb, smult=smult)
+    min_npair = max(0, neleca + nelecb - norb)
+    pairs = range(min_npair, nless + 1)
+    nspins = [neleca + nelecb - 2 * p for p in pairs]
+    if (smult - 1) > nspins[0]:
+        raise ImpossibleSpinError('Maximum possible 2s+1 = {} for ({}e+{}e,{}o)'.format(
+            nspins[0] + 1, neleca, nelecb, norb), norb=norb, neleca=neleca, nelecb=nelecb,
+            smult=smult)
+    dconf = np.array([comb(norb, p) for p in pairs], dtype=np.int64)
+    sconf = np.array([comb(norb - p, ns) for p, ns in zip(pairs, nspins)], dtype=np.int64)
+    ncsf = np.array([count_csfs(ns, smult) for ns in nspins], dtype=np.int64)
+    sizes = dconf * sconf * ncsf
+    offset = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+    return min_npair, offset, dconf, sconf, ncsf
+
+
+def count_all_csfs(norb, neleca, nelecb, smult):
+    a, b, c = get_csfvec_shape(norb, neleca, nelecb, smult)[-3:]
+    return int(np.sum(a * b * c))
+
+
+def addrs2str(nspin, smult, addrs):
+    """Genealogical coupling strings of addresses (csfstring.c:243-293)."""
+    g = csf_gentable(nspin, smult)
+    n1 = (nspin + smult - 1) // 2
+    out = np.zeros(len(addrs), dtype=np.int64)
+    for j, a in enumerate(np.asarray(addrs, dtype=np.int64).tolist()):
+        s, i0, i1 = 1, 0, 0
+        for ispin in range(nspin):
+            if i1 == n1:
+                break
+            if g[i0, i1 + 1] <= a:
+                a -= int(g[i0, i1 + 1])
+                i0 += 1
+            else:
+                s |= 1 << ispin
+                i1 += 1
+        out[j] = s
+    return out
+
+
+def strs2addr(nspin, smult, strs):
+    """Genealogical addresses of coupling strings (csfstring.c:192-240)."""
+    g = csf_gentable(nspin, smult)
+    n1 = (nspin + smult - 1) // 2
+    out = np.zeros(len(strs), dtype=np.int32)
+    for j, s in enumerate(np.asarray(strs, dtype=np.int64).tolist()):
+        a, i0, i1 = 0, 0, 0
+        for ispin in range(nspin):
+            if (s >> ispin) & 1:
+                i1 += 1
+            else:
+                if i1 < n1:
+                    a += int(g[i0, i1 + 1])
+                i0 += 1
+        out[j] = a
+    return out
+
+
+def get_spin_evecs(nspin, neleca, nelecb, smult):
+    """umat[det, csf] of nspin unpaired electrons (csfstring.py:913-960) as a
+    device tensor, bit-identical to FCICSFmakecsf (csfstring.c:86-141)."""
+    assert abs(neleca - nelecb) <= smult - 1
+    assert abs(neleca - nelecb) <= nspin
+    assert abs(neleca - nelecb) % 2 == (smult - 1) % 2
+    assert abs(neleca - nelecb) % 2 == nspin % 2
+    na = (nspin + neleca - nelecb) // 2
+    ndet = comb(nspin, na)
+    ncsf = count_csfs(nspin, smult)
+    umat = torch.empty((ndet, ncsf), dtype=torch.float64, device=device())
+    if ndet * ncsf:
+        _capi.call("csffci_spin_evecs", nspin, neleca, nelecb, smult, ptr(umat), stream())
+    return umat
+
+
+def _block_sign(npair, nelecb):
+    """csfstring.py:623-627."""
+    ncomm = npair * (npair - 1) // 2 + npair * max(0, nelecb - npair)
+    return -1.0 if ncomm % 2 else 1.0
+
+
+class CSFTransformer:
+    """GPU counterpart of csfstring.CSFTransformer (csfstring.py:33-223)."""
+
+    def __init__(self, norb, neleca, nelecb, smult, orbsym=None, wfnsym=None, max_memory=None):
+        require_cuda()
+        if orbsym is not None and wfnsym is not None:
+            raise NotImplementedError("point-group symmetry (csf_symm) is not implemented")
+        self._norb = self._neleca = self._nelecb = self._smult = None
+        self._orbsym = orbsym
+        self.wfnsym = wfnsym
+        self.max_memory = max_memory
+        self._update_spin_cache(norb, neleca, nelecb, smult)
+
+    # ---- cache -----------------------------------------------------------
+    def _update_spin_cache(self, norb, neleca, nelecb, smult):
+        if (self._norb, self._neleca, self._nelecb, self._smult) == (norb, neleca, nelecb, smult):
+            return
+        check_csd_mask_size(norb, neleca, nelecb)
+        min_npair, csf_off, dconf, sconf, ncsf_b = get_csfvec_shape(norb, neleca, nelecb, smult)
+        _, csd_off, _, _, spins = get_csdaddrs_shape(norb, neleca, nelecb)
+        self._norb, self._neleca, self._nelecb, self._smult = norb, neleca, nelecb, smult
+        ndet = comb(norb, neleca) * comb(norb, nelecb)
+        self._ncsf = int(np.sum(dconf * sconf * ncsf_b))
+        dev = device()
+        self.csd_mask = torch.empty(ndet, dtype=torch.int32, device=dev)
+        self.econf_det_mask = torch.empty(ndet, dtype=torch.int32, device=dev)
+        self.econf_csf_mask = torch.empty(max(self._ncsf, 1), dtype=torch.int32, device=dev)
+        _capi.call("csffci_csd_masks", norb, neleca, nelecb, smult, ptr(self.csd_mask),
+                   ptr(self.econf_det_mask), ptr(self.econf_csf_mask), stream())
+        self.econf_csf_mask = self.econf_csf_mask[:self._ncsf]
+        self._blocks = []
+        for ip, npair in enumerate(range(min_npair, min(neleca, nelecb) + 1)):
+            nspin = neleca + nelecb - 2 * npair
+            nc = int(ncsf_b[ip])
+            umat = get_spin_evecs(nspin, neleca, nelecb, smult) if nc > 0 else None
+            self._blocks.append(dict(npair=npair, nspin=nspin, csd_offset=int(csd_off[ip]),
+                                     csf_offset=int(csf_off[ip]), nconf=int(dconf[ip] * sconf[ip]),
+                                     ndet=int(spins[ip]), ncsf=nc,
+                                     sign=_block_sign(npair, nelecb), umat=umat, zmat=None))
+        self._cblocks = None
+        self._eta = None
+        self._shape_info = (min_npair, csf_off, dconf, sconf, ncsf_b)
+
+    def _c_blocks(self, with_zmat=False):
+        if with_zmat:
+            for b in self._blocks:
+                if b["ncsf"] and b["nspin"] >= 2 and b["zmat"] is None:
+                    npos = b["nspin"] * (b["nspin"] - 1) // 2
+                    z = torch.empty((npos, b["ncsf"]), dtype=torch.float64, device=device())
+                    _capi.call("csffci_spin_exchange_table", b["nspin"], self._neleca, self._nelecb,
+                               self._smult, ptr(b["umat"]), ptr(z), stream())
+                    b["zmat"] = z
+        arr = (_capi.Block * len(self._blocks))()
+        for i, b in enumerate(self._blocks):
+            arr[i].csd_offset = b["csd_offset"]
+            arr[i].csf_offset = b["csf_offset"]
+            arr[i].nconf = b["nconf"]
+            arr[i].ndet = b["ndet"]
+            arr[i].ncsf = b["ncsf"]
+            arr[i].nspin = b["nspin"]
+            arr[i].npair = b["npair"]
+            arr[i].sign = b["sign"]
+            arr[i].umat = b["umat"].data_ptr() if b["umat"] is not None and b["umat"].numel() else None
+            arr[i].zmat = b["zmat"].data_ptr() if b["zmat"] is not None else None
+        return arr
+
+    # ---- device transforms ----------------------------------------------
+    def dev_det2csf(self, x):
+        """x: device (nvec, ndet) -> (nvec, ncsf), no normalisation."""
+        x = x.reshape(-1, self.ndet).contiguous()
+        out = torch.empty((x.shape[0], self._ncsf), dtype=torch.float64, device=x.device)
+        blocks = self._c_blocks()
+        _capi.call("csffci_det2csf", x.shape[0], ptr(x), self.ndet, ptr(out), self._ncsf,
+                   ptr(self.csd_mask), blocks, len(self._blocks), stream())
+        return out
+
+    def dev_csf2det(self, x):
+        """x: device (nvec, ncsf) -> (nvec, ndet), no normalisation."""
+        x = x.reshape(-1, self._ncsf).contiguous()
+        out = torch.empty((x.shape[0], self.ndet), dtype=torch.float64, device=x.device)
+        blocks = self._c_blocks()
+        _capi.call("csffci_csf2det", x.shape[0], ptr(x), self._ncsf, ptr(out), self.ndet, self.ndet,
+                   ptr(self.csd_mask), blocks, len(self._blocks), stream())
+        return out
+
+    def dev_hdiag_csf(self, hdiag_det, eri4):
+        out = torch.empty(self._ncsf, dtype=torch.float64, device=device())
+        blocks = self._c_blocks(with_zmat=True)
+        _capi.call("csffci_hdiag_csf", self._norb, self._neleca, self._nelecb, ptr(hdiag_det),
+                   ptr(eri4), ptr(self.csd_mask), blocks, len(self._blocks), ptr(out), stream())
+        return out
+
+    @property
+    def spin_parity(self):
+        """eta with c[Ia,Ib] = eta c[Ib,Ia] for every determinant vector built
+        from CSFs when neleca == nelecb (None otherwise); found once by
+        transforming a probe vector."""
+        if self._neleca != self._nelecb:
+            return None
+        if self._eta is None:
+            g = torch.Generator(device="cpu").manual_seed(7)
+            x = torch.randn(self._ncsf, generator=g, dtype=torch.float64).to(device())
+            c = self.dev_csf2det(x).reshape(self.ndeta, self.ndetb)
+            sym = float(torch.linalg.norm(c - c.T))
+            anti = float(torch.linalg.norm(c + c.T))
+            self._eta = 1 if sym <= anti else -1
+        return self._eta
+
+    # ---- reference-shaped API ------------------------------------------
+    def vec_det2csf(self, civec, order='C', normalize=True, return_norm=False):
+        """csfstring.py:45-52 / transform_civec_det2csf 341-414."""
+        civec, norm = self._transform(civec, order, normalize, reverse=False)
+        if return_norm:
+            return civec, norm
+        return civec
+
+    def vec_csf2det(self, civec, order='C', normalize=True, return_norm=False):
+        """csfstring.py:54-60 / transform_civec_csf2det 416-487."""
+        civec, norm = self._transform(civec, order, normalize, reverse=True)
+        if return_norm:
+            return civec, norm
+        return civec
+
+    def _transform(self, arr, order, normalize, reverse):
+        vec_on_cols = order.upper() == 'F'
+        is_torch = isinstance(arr, torch.Tensor)
+        is_list = isinstance(arr, list)
+        is_tuple = isinstance(arr, tuple)
+        ncol_in = self._ncsf if reverse else self.ndet
+        if is_list or is_tuple:
+            nvec = len(arr)
+            is_flat = False
+            x = torch.stack([to_dev(a).reshape(-1) for a in arr]) if nvec else None
+        else:
+            size = arr.numel() if is_torch else np.asarray(arr).size
+            if reverse and size == 0:
+                return (arr, 0.0)
+            if size % ncol_in != 0:
+                raise ImpossibleCIvecError(
+                    'Impossible CI vector size {0} for system with {1} {2}'.format(
+                        size, ncol_in, 'CSFs' if reverse else 'determinants'),
+                    ndet=self.ndet, norb=self._norb, neleca=self._neleca, nelecb=self._nelecb)
+            nvec = size // ncol_in
+            is_flat = len(arr.shape) == 1
+            x = to_dev(arr)
+        if vec_on_cols:
+            x = x.reshape(ncol_in, nvec).T.contiguous()
+        else:
+            x = x.reshape(nvec, ncol_in)
+        y = self.dev_csf2det(x) if reverse else self.dev_det2csf(x)
+        norm = torch.linalg.norm(y, dim=1)
+        if normalize:
+            if reverse:
+                y = y / norm[:, None]
+            else:
+                ok = ~torch.isclose(norm, torch.zeros_like(norm))
+                y = torch.where(ok[:, None], y / torch.where(ok, norm, torch.ones_like(norm))[:, None], y)
+        if vec_on_cols:
+            y = y.T.contiguous()
+        if not is_torch:
+            y = y.cpu().numpy()
+            norm = norm.cpu().numpy()
+        if is_flat:
+            y = y.reshape(-1)
+        elif is_list:
+            y = list(y)
+        elif is_tuple:
+            y = tuple(y)
+        if norm.shape[0] == 1:
+            norm = norm[0] if not is_torch else norm[0]
+            norm = float(norm)
+        return y, norm
+
+    def mat_det2csf_confspace(self, mat, confs):
+        """transform_opmat_det2csf_pspace (csfstring.py:676-785): an operator
+        given over every determinant of the configurations ``confs`` (ordered
+        configuration by configuration, determinants ascending within each)
+        -> CSF basis over those configurations; returns (op, csf_addrs) with
+        csf_addrs sorted."""
+        from .csf import _pspace_transform
+        return _pspace_transform(self, mat, confs)
+
+    def pack_csf(self, csfvec, order='C'):
+        return csfvec
+
+    def unpack_csf(self, csfvec, order='C'):
+        return csfvec
+
+    def pack_det(self, detvec, order='C'):
+        return detvec
+
+    def unpack_det(self, detvec, order='C'):
+        return detvec
+
+    # ---- properties (setting one triggers a cache update) ---------------
+    @property
+    def norb(self):
+        return self._norb
+
+    @norb.setter
+    def norb(self, x):
+        self._update_spin_cache(x, self._neleca, self._nelecb, self._smult)
+
+    @property
+    def neleca(self):
+        return self._neleca
+
+    @neleca.setter
+    def neleca(self, x):
+        self._update_spin_cache(self._norb, x, self._nelecb, self._smult)
+
+    @property
+    def nelecb(self):
+        return self._nelecb
+
+    @nelecb.setter
+    def nelecb(self, x):
+        self._update_spin_cache(self._norb, self._neleca, x, self._smult)
+
+    @property
+    def smult(self):
+        return self._smult
+
+    @smult.setter
+    def smult(self, x):
+        self._update_spin_cache(self._norb, self._neleca, self._nelecb, x)
+
+    @property
+    def orbsym(self):
+        return self._orbsym
+
+    @property
+    def ndeta(self):
+        return comb(self._norb, self._neleca)
+
+    @property
+    def ndetb(self):
+        return comb(self._norb, self._nelecb)
+
+    @property
+    def ndet(self):
+        return self.ndeta * self.ndetb
+
+    @property
+    def ncsf(self):
+        return self._ncsf
+
+    def print_config(self, printer=print):
+        printer('***** CSFTransformer configuration *****')
+        printer('norb = {}'.format(self.norb))
+        printer('neleca, nelecb = {}, {}'.format(self.neleca, self.nelecb))
+        printer('smult = {}'.format(self.smult))
+        printer('orbsym = {}'.format(self.orbsym))
+        printer('wfnsym = {}'.format(self.wfnsym))
+        printer('ndeta, ndetb = {}, {}'.format(self.ndeta, self.ndetb))
+        printer('ncsf = {}'.format(self.ncsf))
+
+
+def make_econf_csf_mask(norb, neleca, nelecb, smult):
+    """csfstring.py:789-804 on the device."""
+    n = count_all_csfs(norb, neleca, nelecb, smult)
+    mask = torch.empty(max(n, 1), dtype=torch.int32, device=device())
+    _capi.call("csffci_csd_masks", norb, neleca, nelecb, smult, None, None, ptr(mask), stream())
+    return mask[:n]
+
+
+def transform_civec_det2csf(detarr, norb, neleca, nelecb, smult, csd_mask=None, vec_on_cols=False,
+                            do_normalize=True, max_memory=None):
+    t = CSFTransformer(norb, neleca, nelecb, smult)
+    return t._transform(detarr, 'F' if vec_on_cols else 'C', do_normalize, reverse=False)
+
+
+def transform_civec_csf2det(csfarr, norb, neleca, nelecb, smult, csd_mask=None, vec_on_cols=False,
+                            do_normalize=True, max_memory=None):
+    t = CSFTransformer(norb, neleca, nelecb, smult)
+    return t._transform(csfarr, 'F' if vec_on_cols else 'C', do_normalize, reverse=True)

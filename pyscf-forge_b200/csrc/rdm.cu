@@ -1,0 +1,253 @@
+// Reduced density matrices as the adjoint of sigma, and the split-K Gram
+// kernel they share with the Davidson update.
+//
+//   T[pq][J] = <J|E_pq|c>  (gathered through the link tables of J, the same
+//   way sigma builds D, but over all norb^2 ordered pairs)
+//   <bra|E_pq E_rs|ket> = sum_J Tb[qp][J] Tk[rs][J]            (Gram GEMM)
+//   dm1[p][q] = <bra|E_qp|ket>,  dm2[p][q][r][s] = <E_pq E_rs> - d_qr <E_ps>
+// (conventions of pyscf/lib/mcscf/fci_gas.h:260-268).  The determinant
+// space is processed in slabs that fit the caller's workspace, so D(pq,J)
+// is never materialised for the whole space.
+#include "common.cuh"
+
+namespace csffci {
+
+// ---------------------------------------------------------------------------
+// split-K Gram: part[split][i][j] = sum_{k in split} X[i][k] Y[j][k]
+// then out[i][j] (+)= sum_split part[split][i][j] in a fixed order.
+// ---------------------------------------------------------------------------
+constexpr int GT = 32, GK = 32;
+
+__global__ void __launch_bounds__(256) k_gram_part(int nx, const double* __restrict__ x, int64_t ldx,
+                                                   int ny, const double* __restrict__ y, int64_t ldy,
+                                                   int64_t n, int64_t kchunk, int nsplit,
+                                                   double* part) {
+  __shared__ double Xs[GK][GT + 1];
+  __shared__ double Ys[GK][GT + 1];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int tiles_i = (nx + GT - 1) / GT, tiles_j = (ny + GT - 1) / GT;
+  const int64_t ntask = (int64_t)tiles_i * tiles_j * nsplit;
+  for (int64_t task = blockIdx.x; task < ntask; task += gridDim.x) {
+    int split = (int)(task % nsplit);
+    int64_t tt = task / nsplit;
+    int ti = (int)(tt / tiles_j), tj = (int)(tt % tiles_j);
+    int64_t k_begin = split * kchunk, k_end = k_begin + kchunk;
+    if (k_end > n) k_end = n;
+    double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    for (int64_t k0 = k_begin; k0 < k_end; k0 += GK) {
+      for (int e = tid; e < GT * GK; e += 256) {
+        int r = e / GK, kk = e - r * GK;
+        int gi = ti * GT + r, gj = tj * GT + r;
+        int64_t k = k0 + kk;
+        Xs[kk][r] = (gi < nx && k < k_end) ? x[(int64_t)gi * ldx + k] : 0.0;
+        Ys[kk][r] = (gj < ny && k < k_end) ? y[(int64_t)gj * ldy + k] : 0.0;
+      }
+      __syncthreads();
+#pragma unroll 8
+      for (int kk = 0; kk < GK; ++kk) {
+        double a0 = Xs[kk][ty], a1 = Xs[kk][ty + 16];
+        double b0 = Ys[kk][tx], b1 = Ys[kk][tx + 16];
+        acc[0][0] = fma(a0, b0, acc[0][0]);
+        acc[0][1] = fma(a0, b1, acc[0][1]);
+        acc[1][0] = fma(a1, b0, acc[1][0]);
+        acc[1][1] = fma(a1, b1, acc[1][1]);
+      }
+      __syncthreads();
+    }
+    double* P = part + (int64_t)split * nx * ny;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        int gi = ti * GT + ty + 16 * a, gj = tj * GT + tx + 16 * b;
+        if (gi < nx && gj < ny) P[(int64_t)gi * ny + gj] = acc[a][b];
+      }
+  }
+}
+
+__global__ void k_gram_reduce(int nxy, int nsplit, const double* part, double* out, int accumulate) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nxy; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int p = 0; p < nsplit; ++p) s += part[(int64_t)p * nxy + i];
+    out[i] = accumulate ? out[i] + s : s;
+  }
+}
+
+static int gram_nsplit(int nx, int ny, int64_t n) {
+  int tiles = ((nx + GT - 1) / GT) * ((ny + GT - 1) / GT);
+  int64_t want = (148 * 4 + tiles - 1) / tiles;
+  int64_t maxs = (n + 4095) / 4096;
+  if (want > maxs) want = maxs;
+  if (want < 1) want = 1;
+  if (want > 1024) want = 1024;
+  return (int)want;
+}
+
+size_t gram_workspace(int nx, int ny, int64_t n) {
+  return (size_t)gram_nsplit(nx, ny, n) * nx * ny * sizeof(double);
+}
+
+int gram_run(int nx, const double* x, int64_t ldx, int ny, const double* y, int64_t ldy, int64_t n,
+             double* out, int accumulate, double* part, cudaStream_t stream) {
+  int nsplit = gram_nsplit(nx, ny, n);
+  int64_t kchunk = (n + nsplit - 1) / nsplit;
+  kchunk = (kchunk + GK - 1) / GK * GK;
+  nsplit = (int)((n + kchunk - 1) / kchunk);
+  if (nsplit < 1) nsplit = 1;
+  int tiles = ((nx + GT - 1) / GT) * ((ny + GT - 1) / GT);
+  k_gram_part<<<grid_for((int64_t)tiles * nsplit, 1, 148 * 8), 256, 0, stream>>>(
+      nx, x, ldx, ny, y, ldy, n, kchunk, nsplit, part);
+  int st = check_launch("gram");
+  if (st) return st;
+  k_gram_reduce<<<grid_for(nx * ny, 256), 256, 0, stream>>>(nx * ny, nsplit, part, out, accumulate);
+  return check_launch("gram reduce");
+}
+
+// ---------------------------------------------------------------------------
+// T slab: T[pq][j] for determinants J = J0 + j, j < S, pq = p*norb + q
+// ---------------------------------------------------------------------------
+__global__ void k_zero(double* T, long long n) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x)
+    T[t] = 0.0;
+}
+
+__global__ void k_tslab_links(int norb, long long Nb, int nla, int nlb,
+                              const csffci_link_t* __restrict__ la,
+                              const csffci_link_t* __restrict__ lb, const double* __restrict__ c,
+                              long long J0, long long S, int spin, double* T) {
+  const int nl = spin == 0 ? nla : nlb;
+  long long tot = S * nl;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    long long j = t % S;  // consecutive threads -> consecutive determinants
+    int l = (int)(t / S);
+    long long J = J0 + j;
+    long long ja = J / Nb, jb = J - ja * Nb;
+    csffci_link_t e;
+    double v;
+    if (spin == 0) {
+      e = la[ja * nla + l];
+      v = e.sign * c[(long long)e.addr * Nb + jb];
+    } else {
+      e = lb[jb * nlb + l];
+      v = e.sign * c[ja * Nb + e.addr];
+    }
+    int a = e.op & 0xff, i = e.op >> 8;
+    // <J|E_ia|I> = sign for E_ai J = sign I
+    T[(long long)(i * norb + a) * S + j] += v;
+  }
+}
+
+__global__ void k_rdm_assemble(int norb, const double* __restrict__ G, const double* __restrict__ d1,
+                               double* dm2) {
+  const int n = norb, n2 = n * n;
+  long long tot = (long long)n2 * n2;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    int p = (int)(t / ((long long)n * n2));
+    int q = (int)((t / n2) % n);
+    int r = (int)((t / n) % n);
+    int s = (int)(t % n);
+    double v = G[(long long)(q * n + p) * n2 + r * n + s];
+    if (q == r) v -= d1[s * n + p];
+    dm2[t] = v;
+  }
+}
+
+__global__ void k_transpose_small(int n, const double* in, double* out) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n * n; t += gridDim.x * blockDim.x) {
+    int i = t / n, j = t - i * n;
+    out[j * n + i] = in[t];
+  }
+}
+
+}  // namespace csffci
+
+using namespace csffci;
+
+extern "C" {
+
+int csffci_gram(int nx, const double* x, int64_t ldx, int ny, const double* y, int64_t ldy,
+                int64_t n, double* out, void* work, size_t work_bytes, cudaStream_t stream) {
+  CSF_REQUIRE(nx >= 0 && ny >= 0 && n >= 0, "gram: bad sizes");
+  if (nx == 0 || ny == 0) return CSFFCI_OK;
+  size_t need = gram_workspace(nx, ny, n);
+  if (work == nullptr || work_bytes < need) {
+    set_error("gram: workspace of %zu bytes < %zu required", work_bytes, need);
+    return CSFFCI_ERR_MEMORY;
+  }
+  return gram_run(nx, x, ldx, ny, y, ldy, n, out, 0, (double*)work, stream);
+}
+
+size_t csffci_gram_workspace(int nx, int ny, int64_t n) { return gram_workspace(nx, ny, n); }
+
+size_t csffci_rdm12_workspace(int norb, int neleca, int nelecb) {
+  long long ndet = (long long)(host_binom(norb, neleca) * host_binom(norb, nelecb));
+  long long n2 = (long long)norb * norb;
+  long long S = ndet < (1ll << 18) ? ndet : (1ll << 18);
+  if (S < 1) S = 1;
+  size_t t = (size_t)(2 * S * n2) * sizeof(double);
+  size_t g = (size_t)(n2 * n2 + 2 * n2) * sizeof(double);
+  size_t part = gram_workspace((int)n2, (int)n2, S);
+  size_t part1 = gram_workspace(1, (int)n2, S);
+  return t + g + (part > part1 ? part : part1) + 1024;
+}
+
+int csffci_rdm12(int norb, int neleca, int nelecb, const csffci_link_t* link_a,
+                 const csffci_link_t* link_b, const double* bra, const double* ket, double* dm1,
+                 double* dm2, void* work, size_t work_bytes, cudaStream_t stream) {
+  CSF_REQUIRE(norb >= 1 && norb <= 22, "rdm12: norb=%d outside [1,22]", norb);
+  long long Na = (long long)host_binom(norb, neleca), Nb = (long long)host_binom(norb, nelecb);
+  long long ndet = Na * Nb;
+  int n2 = norb * norb;
+  int nla = neleca * (norb - neleca + 1), nlb = nelecb * (norb - nelecb + 1);
+  size_t need = csffci_rdm12_workspace(norb, neleca, nelecb);
+  if (work == nullptr || work_bytes < need) {
+    set_error("rdm12: workspace of %zu bytes < %zu required", work_bytes, need);
+    return CSFFCI_ERR_MEMORY;
+  }
+  long long S = ndet < (1ll << 18) ? ndet : (1ll << 18);
+  double* Tk = (double*)work;
+  double* Tb = Tk + (size_t)S * n2;
+  double* G = Tb + (size_t)S * n2;
+  double* d1t = G + (size_t)n2 * n2;
+  double* part = d1t + 2 * (size_t)n2;
+  const bool same = (bra == ket);
+  int st;
+  for (long long J0 = 0; J0 < ndet; J0 += S) {
+    long long s = (ndet - J0 < S) ? ndet - J0 : S;
+    const int accumulate = J0 > 0;
+    for (int which = 0; which < (same ? 1 : 2); ++which) {
+      double* T = which == 0 ? Tk : Tb;
+      const double* c = which == 0 ? ket : bra;
+      k_zero<<<grid_for(s * n2, 256, 148 * 16), 256, 0, stream>>>(T, s * n2);
+      if ((st = check_launch("rdm T zero"))) return st;
+      if (nla > 0) {
+        k_tslab_links<<<grid_for(s * nla, 256, 148 * 16), 256, 0, stream>>>(
+            norb, Nb, nla, nlb, link_a, link_b, c, J0, s, 0, T);
+        if ((st = check_launch("rdm T alpha"))) return st;
+      }
+      if (nlb > 0) {
+        k_tslab_links<<<grid_for(s * nlb, 256, 148 * 16), 256, 0, stream>>>(
+            norb, Nb, nla, nlb, link_a, link_b, c, J0, s, 1, T);
+        if ((st = check_launch("rdm T beta"))) return st;
+      }
+    }
+    const double* TB = same ? Tk : Tb;
+    // d1t[qp] = sum_J bra_J Tk[qp][J]  -> dm1[p][q] after the transpose
+    if ((st = gram_run(1, bra + J0, s, n2, Tk, s, s, d1t, accumulate, part, stream))) return st;
+    if (dm2) {
+      if ((st = gram_run(n2, TB, s, n2, Tk, s, s, G, accumulate, part, stream))) return st;
+    }
+  }
+  k_transpose_small<<<grid_for(n2, 256), 256, 0, stream>>>(norb, d1t, dm1);
+  if ((st = check_launch("rdm1 transpose"))) return st;
+  if (dm2) {
+    k_rdm_assemble<<<grid_for((long long)n2 * n2, 256, 148 * 8), 256, 0, stream>>>(norb, G, dm1, dm2);
+    return check_launch("rdm2 assemble");
+  }
+  return CSFFCI_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,281 @@
+// det <-> CSF transforms and the CSF diagonal.
+//
+// Per npair block the reference gathers x[:, csd_mask block] into a
+// (nvec*nconf, ndet) matrix, multiplies it by +-umat and scatters into the CSF
+// vector (pyscf/csf_fci/csfstring.py:641-658).  Here each block is one tiled
+// FP64 GEMM whose A-operand loader performs the csd_mask gather (det->CSF)
+// and whose store performs the csd_mask scatter (CSF->det); csd_mask is a
+// permutation, so the scatter has no conflicts.  HBM-bound: every CI element
+// is read once and written once per call.
+#include "common.cuh"
+
+namespace csffci {
+
+enum { MODE_DET2CSF = 0, MODE_CSF2DET = 1 };
+
+struct BlockGemmArgs {
+  const double* x;
+  double* y;
+  int64_t ldx, ldy;
+  const uint32_t* mask;
+  const double* umat;
+  int64_t csd_off, csf_off, nconf;
+  int ndet, ncsf;
+  int nvec;
+  double sign;
+};
+
+constexpr int TBM = 64, TBN = 64, TBK = 16;
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_block_gemm(BlockGemmArgs g) {
+  __shared__ double As[TBK][TBM + 1];
+  __shared__ double Bs[TBK][TBN + 1];
+  const int64_t M = (int64_t)g.nvec * g.nconf;
+  const int N = (MODE == MODE_DET2CSF) ? g.ncsf : g.ndet;
+  const int K = (MODE == MODE_DET2CSF) ? g.ndet : g.ncsf;
+  const int tid = threadIdx.x;
+  const int tx = tid & 15, ty = tid >> 4;
+  const int64_t ntile_m = (M + TBM - 1) / TBM;
+  const int ntile_n = (N + TBN - 1) / TBN;
+  for (int64_t tile = blockIdx.x; tile < ntile_m * ntile_n; tile += gridDim.x) {
+    const int64_t m0 = (tile / ntile_n) * TBM;
+    const int n0 = (int)(tile % ntile_n) * TBN;
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    for (int k0 = 0; k0 < K; k0 += TBK) {
+      // A tile: 64 rows x 16 k; thread loads (row = tid/16 + 16*r, k = tid%16)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        int row = ty + 16 * r;
+        int kk = tx;
+        int64_t m = m0 + row;
+        double v = 0.0;
+        if (m < M && k0 + kk < K) {
+          int64_t vec = m / g.nconf, conf = m - vec * g.nconf;
+          if (MODE == MODE_DET2CSF) {
+            uint32_t d = g.mask[g.csd_off + conf * g.ndet + k0 + kk];
+            v = g.x[vec * g.ldx + d];
+          } else {
+            v = g.x[vec * g.ldx + g.csf_off + conf * g.ncsf + k0 + kk];
+          }
+        }
+        As[kk][row] = v;
+      }
+      // B tile: 16 k x 64 n
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        double v = 0.0;
+        if (MODE == MODE_DET2CSF) {
+          int kk = ty, col = tx + 16 * r;
+          if (k0 + kk < K && n0 + col < N) v = g.umat[(int64_t)(k0 + kk) * g.ncsf + n0 + col];
+          Bs[kk][col] = v;
+        } else {
+          int kk = tx, col = ty + 16 * r;
+          if (k0 + kk < K && n0 + col < N) v = g.umat[(int64_t)(n0 + col) * g.ncsf + k0 + kk];
+          Bs[kk][col] = v;
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int kk = 0; kk < TBK; ++kk) {
+        double a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      int64_t m = m0 + ty * 4 + i;
+      if (m >= M) continue;
+      int64_t vec = m / g.nconf, conf = m - vec * g.nconf;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        int n = n0 + tx * 4 + j;
+        if (n >= N) continue;
+        double v = g.sign * acc[i][j];
+        if (MODE == MODE_DET2CSF) {
+          g.y[vec * g.ldy + g.csf_off + conf * g.ncsf + n] = v;
+        } else {
+          uint32_t d = g.mask[g.csd_off + conf * g.ndet + n];
+          g.y[vec * g.ldy + d] = v;
+        }
+      }
+    }
+  }
+}
+
+__global__ void k_zero_rows(double* y, int64_t ldy, int nvec, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)nvec * n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t v = i / n;
+    y[v * ldy + (i - v * n)] = 0.0;
+  }
+}
+
+template <int MODE>
+static int run_blocks(int nvec, const double* x, int64_t ldx, double* y, int64_t ldy,
+                      const uint32_t* mask, const csffci_block_t* blocks, int nblock,
+                      cudaStream_t stream) {
+  for (int b = 0; b < nblock; ++b) {
+    const csffci_block_t& B = blocks[b];
+    if (B.ncsf == 0 || B.nconf == 0) continue;
+    CSF_REQUIRE(B.umat != nullptr, "transform: block %d has no umat", b);
+    BlockGemmArgs g;
+    g.x = x;
+    g.y = y;
+    g.ldx = ldx;
+    g.ldy = ldy;
+    g.mask = mask;
+    g.umat = B.umat;
+    g.csd_off = B.csd_offset;
+    g.csf_off = B.csf_offset;
+    g.nconf = B.nconf;
+    g.ndet = B.ndet;
+    g.ncsf = B.ncsf;
+    g.nvec = nvec;
+    g.sign = B.sign;
+    int64_t M = (int64_t)nvec * B.nconf;
+    int N = (MODE == MODE_DET2CSF) ? B.ncsf : B.ndet;
+    int64_t tiles = ((M + TBM - 1) / TBM) * ((N + TBN - 1) / TBN);
+    k_block_gemm<MODE><<<grid_for(tiles, 1, 148 * 8), 256, 0, stream>>>(g);
+    int st = check_launch("det/csf transform");
+    if (st) return st;
+  }
+  return CSFFCI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// CSF diagonal: per configuration c and CSF k
+//   hdiag_csf[c,k] = sum_x U[x,k]^2 hdiag_det[x] + sum_{a<b} K(S_a,S_b) Z[ab,k]
+// which equals sum_xy U[x,k] H_xy U[y,k] over the within-configuration block
+// of pyscf/lib/csf/csfstring.c:295-362 (H_xy = (-1)^(somos between)
+// (pq|qp) for two dets that differ by exchanging the spins of SOMOs p,q);
+// K(p,q) = (pq|qp) = eri[pq][pq].
+// ---------------------------------------------------------------------------
+
+struct HdiagCsfArgs {
+  const double* hd;
+  const double* eri;
+  const uint32_t* mask;
+  const double* umat;
+  const double* zmat;
+  double* out;
+  int64_t csd_off, csf_off, nconf, sconf;
+  int ndet, ncsf, nspin, npair, norb, npair_orb;
+};
+
+__global__ void k_hdiag_csf(HdiagCsfArgs g) {
+  const int64_t n = g.nconf * g.ncsf;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t conf = i / g.ncsf;
+    int k = (int)(i - conf * g.ncsf);
+    double acc = 0.0;
+    const uint32_t* m = g.mask + g.csd_off + conf * g.ndet;
+    for (int x = 0; x < g.ndet; ++x) {
+      double u = g.umat[(int64_t)x * g.ncsf + k];
+      acc = fma(u * u, g.hd[m[x]], acc);
+    }
+    if (g.nspin >= 2) {
+      int64_t dc = conf / g.sconf, sc = conf - dc * g.sconf;
+      unsigned long long dstr = str_unrank(g.norb, g.npair, (unsigned long long)dc);
+      unsigned long long sstr = str_unrank(g.norb - g.npair, g.nspin, (unsigned long long)sc);
+      int somo[64];
+      int ns = 0, isorb = 0;
+      for (int iorb = 0; iorb < g.norb; ++iorb) {
+        if ((dstr >> iorb) & 1ull) continue;
+        if ((sstr >> isorb) & 1ull) somo[ns++] = iorb;
+        ++isorb;
+      }
+      int ab = 0;
+      for (int b = 1; b < ns; ++b)
+        for (int a = 0; a < b; ++a, ++ab) {
+          int pq = pair_index(somo[a], somo[b]);
+          acc = fma(g.eri[(int64_t)pq * g.npair_orb + pq], g.zmat[(int64_t)ab * g.ncsf + k], acc);
+        }
+    }
+    g.out[g.csf_off + conf * g.ncsf + k] = acc;
+  }
+}
+
+}  // namespace csffci
+
+using namespace csffci;
+
+extern "C" {
+
+int csffci_det2csf(int nvec, const double* x_det, int64_t ld_det, double* x_csf, int64_t ld_csf,
+                   const uint32_t* csd_mask, const csffci_block_t* blocks, int nblock,
+                   cudaStream_t stream) {
+  CSF_REQUIRE(nvec >= 0 && blocks != nullptr && nblock >= 0, "det2csf: bad arguments");
+  if (nvec == 0) return CSFFCI_OK;
+  return run_blocks<MODE_DET2CSF>(nvec, x_det, ld_det, x_csf, ld_csf, csd_mask, blocks, nblock,
+                                  stream);
+}
+
+int csffci_csf2det(int nvec, const double* x_csf, int64_t ld_csf, double* x_det, int64_t ld_det,
+                   int64_t ndet, const uint32_t* csd_mask, const csffci_block_t* blocks,
+                   int nblock, cudaStream_t stream) {
+  CSF_REQUIRE(nvec >= 0 && blocks != nullptr && nblock >= 0, "csf2det: bad arguments");
+  if (nvec == 0) return CSFFCI_OK;
+  // determinants of blocks without CSFs (and every other one, for
+  // simplicity of the contract) start from zero
+  bool full = true;
+  for (int b = 0; b < nblock; ++b)
+    if (blocks[b].ncsf == 0 && blocks[b].nconf > 0) full = false;
+  if (!full) {
+    k_zero_rows<<<grid_for((int64_t)nvec * ndet, 256, 148 * 16), 256, 0, stream>>>(x_det, ld_det,
+                                                                                     nvec, ndet);
+    int st = check_launch("csf2det zero");
+    if (st) return st;
+  }
+  return run_blocks<MODE_CSF2DET>(nvec, x_csf, ld_csf, x_det, ld_det, csd_mask, blocks, nblock,
+                                  stream);
+}
+
+int csffci_hdiag_csf(int norb, int neleca, int nelecb, const double* hdiag_det, const double* eri,
+                     const uint32_t* csd_mask, const csffci_block_t* blocks, int nblock,
+                     double* hdiag_csf, cudaStream_t stream) {
+  CSF_REQUIRE(norb >= 0 && norb <= 63 && blocks != nullptr, "hdiag_csf: bad arguments");
+  int npair_orb = norb * (norb + 1) / 2;
+  for (int b = 0; b < nblock; ++b) {
+    const csffci_block_t& B = blocks[b];
+    if (B.ncsf == 0 || B.nconf == 0) continue;
+    CSF_REQUIRE(B.umat != nullptr, "hdiag_csf: block %d has no umat", b);
+    CSF_REQUIRE(B.nspin < 2 || B.zmat != nullptr, "hdiag_csf: block %d has no zmat", b);
+    HdiagCsfArgs g;
+    g.hd = hdiag_det;
+    g.eri = eri;
+    g.mask = csd_mask;
+    g.umat = B.umat;
+    g.zmat = B.zmat;
+    g.out = hdiag_csf;
+    g.csd_off = B.csd_offset;
+    g.csf_off = B.csf_offset;
+    g.nconf = B.nconf;
+    g.sconf = (int64_t)host_binom(norb - B.npair, B.nspin);
+    g.ndet = B.ndet;
+    g.ncsf = B.ncsf;
+    g.nspin = B.nspin;
+    g.npair = B.npair;
+    g.norb = norb;
+    g.npair_orb = npair_orb;
+    k_hdiag_csf<<<grid_for(B.nconf * B.ncsf, 128, 148 * 32), 128, 0, stream>>>(g);
+    int st = check_launch("hdiag_csf");
+    if (st) return st;
+  }
+  return CSFFCI_OK;
+}
+
+}  // extern "C"

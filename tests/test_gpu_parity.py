@@ -1,0 +1,344 @@
+"""GPU parity: every kernel of the CSF-FCI path against the golden fixtures
+(generated from the reference) and the oracle (reference C in oracle/_ref
+and the numpy restatement).  Integer maps must be bit-exact; floating-point
+results use the tolerances stated next to each assertion."""
+import hashlib
+
+import numpy as np
+import pytest
+import torch
+
+import gasref
+import restate as R
+from conftest import load_golden, seeded_integrals
+
+pytestmark = pytest.mark.gpu
+
+needs_ref = pytest.mark.skipif(not gasref.available(), reason="oracle/_ref not built")
+
+
+def _mods():
+    import pyscf_forge_b200 as P
+    from pyscf_forge_b200.fci import direct_spin1 as D
+    from pyscf_forge_b200.csf_fci import csfstring as C
+    return P, D, C
+
+
+def _case(g):
+    return int(g["norb"]), int(g["neleca"]), int(g["nelecb"]), int(g["smult"])
+
+
+def test_link_tables_bit_exact(golden_case):
+    P, D, C = _mods()
+    n, na, nb, sm = _case(golden_case)
+    assert np.array_equal(D.decode_link_table(D.dev_link_table(n, na))[:, :golden_case["link_a"].shape[1]],
+                          golden_case["link_a"])
+    assert np.array_equal(D.decode_link_table(D.dev_link_table(n, nb))[:, :golden_case["link_b"].shape[1]],
+                          golden_case["link_b"])
+
+
+@needs_ref
+@pytest.mark.parametrize("norb,nelec", [(12, 6), (16, 8), (14, 5), (9, 1)])
+def test_link_tables_vs_reference_c(norb, nelec):
+    _, D, _ = _mods()
+    sp = gasref.CASSpace(norb, (nelec, nelec))
+    ref = sp.raw_link_table(0)
+    sp.close()
+    assert np.array_equal(D.decode_link_table(D.dev_link_table(norb, nelec)), ref)
+
+
+def test_masks_bit_exact(golden_case):
+    _, _, C = _mods()
+    n, na, nb, sm = _case(golden_case)
+    t = C.CSFTransformer(n, na, nb, sm)
+    assert np.array_equal(t.csd_mask.cpu().numpy().view(np.uint32), golden_case["csd_mask"])
+    assert np.array_equal(t.econf_det_mask.cpu().numpy().view(np.uint32), golden_case["econf_det_mask"])
+    assert np.array_equal(t.econf_csf_mask.cpu().numpy().view(np.uint32), golden_case["econf_csf_mask"])
+
+
+def _sha(t):
+    return hashlib.sha256(np.ascontiguousarray(t.cpu().numpy().view(np.uint32)).tobytes()).hexdigest()
+
+
+def test_masks_c1_bit_exact():
+    _, _, C = _mods()
+    g = load_golden("c1_norb12_6e6e_s0")
+    t = C.CSFTransformer(12, 6, 6, 1)
+    assert _sha(t.csd_mask) == str(g["sha_csd_mask"])
+    assert _sha(t.econf_det_mask) == str(g["sha_econf_det_mask"])
+    assert _sha(t.econf_csf_mask) == str(g["sha_econf_csf_mask"])
+
+
+def test_masks_permutation_large():
+    """norb=16 (8,8): csd_mask is a permutation and econf_det_mask inverts it
+    blockwise (size-independent properties at the full size)."""
+    _, _, C = _mods()
+    t = C.CSFTransformer(16, 8, 8, 1)
+    m = t.csd_mask.long()
+    n = m.numel()
+    assert n == 165636900
+    seen = torch.zeros(n, dtype=torch.int8, device=m.device)
+    seen[m] = 1
+    assert int(seen.sum()) == n
+    assert t.ncsf == 34763300
+    del seen
+
+
+@needs_ref
+def test_spin_evecs_bit_exact():
+    _, _, C = _mods()
+    for nspin in range(0, 13):
+        for na in range(0, nspin + 1):
+            nb = nspin - na
+            for smult in range(abs(na - nb) + 1, nspin + 2, 2):
+                u = C.get_spin_evecs(nspin, na, nb, smult).cpu().numpy()
+                det = R.addrs2str(nspin, na, np.arange(u.shape[0]))
+                coup = R.gen_addrs2str(nspin, smult, np.arange(u.shape[1]))
+                ref = gasref.makecsf(det, coup, nspin, smult - 1, na - nb)
+                assert np.array_equal(u, ref), (nspin, na, nb, smult)
+
+
+def test_spin_evecs_fixture(golden_case):
+    _, _, C = _mods()
+    n, na, nb, sm = _case(golden_case)
+    for key in golden_case:
+        if key.startswith("umat_"):
+            nspin = int(key.split("_")[1])
+            assert np.array_equal(C.get_spin_evecs(nspin, na, nb, sm).cpu().numpy(), golden_case[key])
+
+
+def test_spin_evecs_orthonormal_s2():
+    """test_csfstring.py:7-37: umat orthonormal and diagonalises S^2 (from
+    FCICSFmakeS2mat) with eigenvalue S(S+1); tolerance 1e-8 as there."""
+    if not gasref.available():
+        pytest.skip("oracle/_ref not built")
+    _, _, C = _mods()
+    for nspin in range(1, 11):
+        for twoms in range(nspin % 2, nspin + 1, 2):
+            na = (nspin + twoms) // 2
+            nb = nspin - na
+            det = R.addrs2str(nspin, na, np.arange(R.num_strings(nspin, na)))
+            s2 = gasref.makeS2mat(det, nspin, twoms)
+            for smult in range(twoms + 1, nspin + 2, 2):
+                u = C.get_spin_evecs(nspin, na, nb, smult).cpu().numpy()
+                s = (smult - 1) / 2
+                assert np.linalg.norm(u.T @ u - np.eye(u.shape[1])) < 1e-8
+                assert np.linalg.norm(u.T @ s2 @ u - s * (s + 1) * np.eye(u.shape[1])) < 1e-8
+
+
+def test_transforms(golden_case):
+    _, _, C = _mods()
+    n, na, nb, sm = _case(golden_case)
+    t = C.CSFTransformer(n, na, nb, sm)
+    # tolerance 1e-13: same sums as the reference in a different order
+    np.testing.assert_allclose(t.vec_det2csf(golden_case["ci_rand"], normalize=False),
+                               golden_case["det2csf_rand"], atol=1e-13)
+    np.testing.assert_allclose(t.vec_csf2det(golden_case["csf_rand"], normalize=False),
+                               golden_case["csf2det_rand"], atol=1e-13)
+    # batched, list and column layouts follow the reference shapes
+    xs = [golden_case["ci_rand"], 2.0 * golden_case["ci_rand"]]
+    out = t.vec_det2csf(xs, normalize=False)
+    assert isinstance(out, list) and len(out) == 2
+    np.testing.assert_allclose(out[1], 2.0 * golden_case["det2csf_rand"], atol=1e-12)
+    cols = t.vec_det2csf(np.stack(xs, axis=1), order='F', normalize=False)
+    np.testing.assert_allclose(cols[:, 0], golden_case["det2csf_rand"], atol=1e-13)
+
+
+def test_round_trip_c1():
+    """det -> csf -> det is a projector: csf2det(det2csf(x)) applied twice is
+    idempotent, and csf -> det -> csf is the identity (full size C1)."""
+    _, _, C = _mods()
+    t = C.CSFTransformer(12, 6, 6, 1)
+    g = torch.Generator(device="cpu").manual_seed(0)
+    x = torch.randn(2, t.ncsf, generator=g, dtype=torch.float64).cuda()
+    y = t.dev_det2csf(t.dev_csf2det(x))
+    torch.testing.assert_close(y, x, atol=1e-12, rtol=0)
+
+
+def test_diagonals_and_absorb(golden_case):
+    P, D, C = _mods()
+    n, na, nb, sm = _case(golden_case)
+    h1, eri = golden_case["h1"], golden_case["eri"]
+    sol = P.csf_solver(None, smult=sm)
+    hd = sol.make_hdiag(h1, eri, n, (na, nb))
+    np.testing.assert_allclose(hd, golden_case["hdiag_det"], atol=1e-12)
+    hc = sol.make_hdiag_csf(h1, eri, n, (na, nb))
+    np.testing.assert_allclose(hc, golden_case["hdiag_csf"], atol=1e-12)
+    h2e = D.absorb_h1e(h1, eri, n, (na, nb), 0.5)
+    np.testing.assert_allclose(h2e, golden_case["h2e"], atol=1e-13)
+
+
+def test_sigma_golden(golden_case):
+    P, D, C = _mods()
+    n, na, nb, sm = _case(golden_case)
+    # 1e-11: the reference's own GAS-vs-direct_spin1 tolerance (test_gasci.py:285-290)
+    sig = D.contract_2e(golden_case["h2e"], golden_case["ci_rand"], n, (na, nb))
+    np.testing.assert_allclose(sig, golden_case["sigma_rand"], atol=1e-11)
+
+
+@needs_ref
+@pytest.mark.parametrize("norb,nelec,rank", [(10, (5, 4), 12), (11, (3, 6), 10), (12, (6, 6), 24),
+                                             (9, (9, 2), 8), (13, (2, 2), 8)])
+def test_sigma_vs_reference_c(norb, nelec, rank):
+    _, D, _ = _mods()
+    h1, eri = seeded_integrals(norb, rank, seed=5)
+    h2e = R.absorb_h1e(h1, eri, norb, nelec, 0.5)
+    rng = np.random.default_rng(6)
+    ci = rng.normal(size=R.num_strings(norb, nelec[0]) * R.num_strings(norb, nelec[1]))
+    ci /= np.linalg.norm(ci)
+    ref = gasref.contract_2e(h2e, ci, norb, nelec)
+    got = D.contract_2e(h2e, ci, norb, nelec)
+    np.testing.assert_allclose(got, ref, atol=1e-10)  # sigma tolerance 1e-9 of the target, tighter here
+
+
+def test_sigma_c1_fixture():
+    _, D, _ = _mods()
+    g = load_golden("c1_norb12_6e6e_s0")
+    h1, eri = seeded_integrals(12, 24)
+    h2e = R.absorb_h1e(h1, eri, 12, (6, 6), 0.5)
+    rng = np.random.default_rng(1)
+    ci = rng.normal(size=924 * 924)
+    ci /= np.linalg.norm(ci)
+    sig = D.contract_2e(h2e, ci, 12, (6, 6))
+    np.testing.assert_allclose(sig[:64], g["sigma_rand_head"], atol=1e-11)
+    fp = float(np.dot(np.cos(np.arange(sig.size)), sig))
+    assert abs(fp - float(g["fp_sigma_rand"])) < 1e-8
+
+
+@pytest.mark.parametrize("norb,nelec,smult", [(8, (4, 4), 1), (8, (4, 4), 3), (10, (5, 5), 1),
+                                              (9, (3, 3), 5)])
+def test_sigma_spin_symmetric_mode(norb, nelec, smult):
+    """The row-local kernel + transpose-add equals the general kernel for
+    vectors built from CSFs (c = eta c^T)."""
+    _, D, C = _mods()
+    t = C.CSFTransformer(norb, nelec[0], nelec[1], smult)
+    h1, eri = seeded_integrals(norb, 8, seed=2)
+    h2e = D.dev_absorb_h1e(h1, R.restore4(eri, norb), norb, nelec, 0.5)
+    g = torch.Generator(device="cpu").manual_seed(1)
+    x = torch.randn(t.ncsf, generator=g, dtype=torch.float64).cuda()
+    c = t.dev_csf2det(x)[0]
+    eta = t.spin_parity
+    assert eta in (1, -1)
+    ref = D.dev_contract_2e(h2e, c, norb, nelec)
+    got = D.dev_contract_2e(h2e, c, norb, nelec, eta=eta)
+    torch.testing.assert_close(got, ref, atol=1e-11, rtol=0)
+
+
+def test_contract_1e():
+    _, D, _ = _mods()
+    norb, nelec = 7, (4, 2)
+    rng = np.random.default_rng(3)
+    ha = rng.normal(size=(norb, norb))
+    hb = rng.normal(size=(norb, norb))
+    ci = rng.normal(size=R.num_strings(norb, 4) * R.num_strings(norb, 2))
+    got = D.contract_1e(np.array([ha, hb]), ci, norb, nelec)
+    ref = R.contract_1e_ab(ha, hb, ci, norb, nelec)
+    np.testing.assert_allclose(got, ref, atol=1e-12)
+
+
+def test_rdms_golden(golden_case):
+    P, D, C = _mods()
+    if "rdm1" not in golden_case:
+        pytest.skip("no solve in this fixture")
+    n, na, nb, sm = _case(golden_case)
+    c = golden_case["ci_roots"][0]
+    dm1, dm2 = D.make_rdm12(c, n, (na, nb))
+    # 1e-12 as test_gasci.py:765-786 (RDM target 1e-8)
+    np.testing.assert_allclose(dm1, golden_case["rdm1"], atol=1e-12)
+    np.testing.assert_allclose(dm2, golden_case["rdm2"], atol=1e-12)
+
+
+@needs_ref
+@pytest.mark.parametrize("norb,nelec", [(6, (3, 3)), (8, (5, 3)), (10, (4, 4))])
+def test_trans_rdm_vs_reference_c(norb, nelec):
+    _, D, _ = _mods()
+    rng = np.random.default_rng(8)
+    nd = R.num_strings(norb, nelec[0]) * R.num_strings(norb, nelec[1])
+    bra = rng.normal(size=nd)
+    ket = rng.normal(size=nd)
+    bra /= np.linalg.norm(bra)
+    ket /= np.linalg.norm(ket)
+    d1, d2 = D.trans_rdm12(bra, ket, norb, nelec)
+    e1, e2 = gasref.make_rdm12(bra, ket, norb, nelec)
+    np.testing.assert_allclose(d1, e1, atol=1e-12)
+    np.testing.assert_allclose(d2, e2, atol=1e-12)
+
+
+def _dense_csf_columns(g, addr):
+    """<csf_i|H|csf_j> for j in addr through the reference C sigma."""
+    n, na, nb, sm = _case(g)
+    plan = gasref.SigmaPlan(n, (na, nb), g["h2e"])
+    ncsf = g["hdiag_csf"].size
+    cols = []
+    for j in addr:
+        x = np.zeros(ncsf)
+        x[j] = 1.0
+        d = R.transform_det2csf(x, n, na, nb, sm, csd_mask=g["csd_mask"], reverse=True)[0]
+        cols.append(R.transform_det2csf(plan(d), n, na, nb, sm, csd_mask=g["csd_mask"])[0])
+    plan.close()
+    return np.array(cols).T
+
+
+@needs_ref
+def test_pspace(golden_case):
+    P, _, _ = _mods()
+    n, na, nb, sm = _case(golden_case)
+    sol = P.csf_solver(None, smult=sm)
+    addr, h0 = sol.pspace(golden_case["h1"], golden_case["eri"], n, (na, nb), npsp=200)
+    assert len(set(addr.tolist())) == len(addr)
+    H = _dense_csf_columns(golden_case, addr)
+    np.testing.assert_allclose(h0, H[addr], atol=1e-11)
+    if np.array_equal(np.sort(addr), golden_case["pspace_addr"]):
+        o = np.argsort(addr)
+        np.testing.assert_allclose(h0[np.ix_(o, o)], golden_case["pspace_h0"], atol=1e-11)
+
+
+def test_kernel_energies(golden_case):
+    P, _, _ = _mods()
+    if "energies" not in golden_case:
+        pytest.skip("no solve in this fixture")
+    n, na, nb, sm = _case(golden_case)
+    nroots = int(golden_case["nroots"])
+    for davidson_only in (False, True):
+        sol = P.csf_solver(None, smult=sm)
+        sol.nroots = nroots
+        sol.davidson_only = davidson_only
+        e, ci = sol.kernel(golden_case["h1"], golden_case["eri"], n, (na, nb))
+        e = np.atleast_1d(e)
+        # energies within 1e-9 Eh of the reference CPU CSFFCISolver
+        np.testing.assert_allclose(e, golden_case["energies"], atol=1e-9)
+        cis = ci if isinstance(ci, list) else [ci]
+        for k, c in enumerate(cis):
+            ref = golden_case["ci_roots"][k]
+            ov = abs(float(np.dot(c.ravel(), ref)))
+            assert ov > 1 - 1e-7
+            ss, m = R.spin_square(c, n, (na, nb))
+            assert abs(m - sm) < 1e-6
+
+
+def test_kernel_c1_three_roots():
+    P, _, _ = _mods()
+    g = load_golden("c1_norb12_6e6e_s0")
+    h1, eri = seeded_integrals(12, 24)
+    sol = P.csf_solver(None, smult=1)
+    sol.nroots = 3
+    e, ci = sol.kernel(h1, eri, 12, (6, 6))
+    np.testing.assert_allclose(e, g["energies"], atol=1e-9)
+    dm1, dm2 = sol.make_rdm12(ci[0], 12, (6, 6))
+    np.testing.assert_allclose(dm1, g["rdm1_root0"], atol=1e-8)
+    fp = float(np.dot(np.cos(np.arange(dm2.size)), dm2.ravel()))
+    assert abs(fp - float(g["fp_rdm2_root0"])) < 1e-6
+
+
+def test_errors_are_raised():
+    P, D, C = _mods()
+    from pyscf_forge_b200 import _capi
+    with pytest.raises(C.ImpossibleSpinError):
+        C.CSFTransformer(6, 3, 1, 1)
+    with pytest.raises(_capi.CSFFCIError):
+        _capi.call("csffci_sigma", 40, 2, 2, None, None, None, None, None, 0, 1, None, 0, None)
+    with pytest.raises(MemoryError):
+        _capi.call("csffci_hdiag_det", 6, 3, 3, None, None, None, None, None, 16, None)
+    t = C.CSFTransformer(6, 3, 3, 1)
+    with pytest.raises(C.ImpossibleCIvecError):
+        t.vec_det2csf(np.zeros(17))

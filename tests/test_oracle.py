@@ -1,0 +1,115 @@
+"""CPU: the numpy restatement (oracle/restate.py) against the golden
+fixtures generated from the reference itself, and against the reference's
+own C built into oracle/_ref."""
+import numpy as np
+import pytest
+
+import restate as R
+import gasref
+from conftest import load_golden, seeded_integrals
+
+needs_ref = pytest.mark.skipif(not gasref.available(), reason="oracle/_ref not built")
+
+
+def test_masks_and_links(golden_case):
+    g = golden_case
+    n, na, nb, sm = int(g["norb"]), int(g["neleca"]), int(g["nelecb"]), int(g["smult"])
+    csd = R.make_csd_mask(n, na, nb)
+    assert np.array_equal(csd, g["csd_mask"])
+    assert np.array_equal(R.make_econf_det_mask(n, na, nb, csd), g["econf_det_mask"])
+    assert np.array_equal(R.make_econf_csf_mask(n, na, nb, sm), g["econf_csf_mask"])
+    assert np.array_equal(R.link_table(n, na), g["link_a"])
+    assert np.array_equal(R.link_table(n, nb), g["link_b"])
+
+
+def test_transforms_and_diagonals(golden_case):
+    g = golden_case
+    n, na, nb, sm = int(g["norb"]), int(g["neleca"]), int(g["nelecb"]), int(g["smult"])
+    h1, eri = g["h1"], g["eri"]
+    np.testing.assert_allclose(R.make_hdiag(h1, eri, n, (na, nb)), g["hdiag_det"], atol=1e-12)
+    np.testing.assert_allclose(R.make_hdiag_csf(h1, eri, n, (na, nb), sm), g["hdiag_csf"], atol=1e-12)
+    np.testing.assert_allclose(R.absorb_h1e(h1, eri, n, (na, nb), 0.5), g["h2e"], atol=1e-13)
+    np.testing.assert_allclose(R.transform_det2csf(g["ci_rand"], n, na, nb, sm)[0], g["det2csf_rand"],
+                               atol=1e-13)
+    np.testing.assert_allclose(R.transform_det2csf(g["csf_rand"], n, na, nb, sm, reverse=True)[0],
+                               g["csf2det_rand"], atol=1e-13)
+    for key in g:
+        if key.startswith("umat_"):
+            nspin = int(key.split("_")[1])
+            assert np.array_equal(R.get_spin_evecs(nspin, na, nb, sm), g[key])
+
+
+def test_sigma_and_rdms(golden_case):
+    g = golden_case
+    n, na, nb = int(g["norb"]), int(g["neleca"]), int(g["nelecb"])
+    sig = R.contract_2e(g["h2e"], g["ci_rand"], n, (na, nb))
+    np.testing.assert_allclose(sig, g["sigma_rand"], atol=1e-11)
+    if "rdm1" in g:
+        c = g["ci_roots"][0]
+        d1, d2 = R.make_rdm12(c, c, n, (na, nb))
+        np.testing.assert_allclose(d1, g["rdm1"], atol=1e-12)
+        np.testing.assert_allclose(d2, g["rdm2"], atol=1e-12)
+
+
+def test_pspace_and_energy(golden_case):
+    g = golden_case
+    n, na, nb, sm = int(g["norb"]), int(g["neleca"]), int(g["nelecb"]), int(g["smult"])
+    if g["hdiag_det"].size > 1300:
+        pytest.skip("dense check is sized for the small cases")
+    h2e = g["h2e"]
+    nd = g["hdiag_det"].size
+    H = np.array([R.contract_2e(h2e, np.eye(nd)[i], n, (na, nb)) for i in range(nd)])
+    Hc = R.transform_det2csf(H, n, na, nb, sm)
+    Hc = R.transform_det2csf(Hc.T, n, na, nb, sm)
+    addr = g["pspace_addr"]
+    np.testing.assert_allclose(g["pspace_h0"], Hc[np.ix_(addr, addr)], atol=1e-11)
+    if "energies" in g:
+        w = np.linalg.eigvalsh(Hc)
+        np.testing.assert_allclose(g["energies"], w[:len(g["energies"])], atol=1e-9)
+
+
+@needs_ref
+@pytest.mark.parametrize("norb,nelec", [(6, (3, 3)), (7, (4, 2)), (8, (3, 5))])
+def test_restatement_vs_reference_c(norb, nelec):
+    h1, eri = seeded_integrals(norb, 10, seed=3)
+    h2e = R.absorb_h1e(h1, eri, norb, nelec, 0.5)
+    rng = np.random.default_rng(4)
+    ci = rng.normal(size=R.num_strings(norb, nelec[0]) * R.num_strings(norb, nelec[1]))
+    np.testing.assert_allclose(R.contract_2e(h2e, ci, norb, nelec), gasref.contract_2e(h2e, ci, norb, nelec),
+                               atol=1e-11)
+    np.testing.assert_allclose(R.make_hdiag(h1, eri, norb, nelec), gasref.make_hdiag(h1, eri, norb, nelec),
+                               atol=1e-12)
+    ket = rng.normal(size=ci.size)
+    d1, d2 = R.make_rdm12(ci, ket, norb, nelec)
+    e1, e2 = gasref.make_rdm12(ci, ket, norb, nelec)
+    np.testing.assert_allclose(d1, e1, atol=1e-11)
+    np.testing.assert_allclose(d2, e2, atol=1e-11)
+    sp = gasref.CASSpace(norb, nelec)
+    la = sp.raw_link_table(0)
+    sp.close()
+    assert np.array_equal(la, R.link_table(norb, nelec[0])) or np.array_equal(la, R.link_table(norb, nelec[1]))
+
+
+@needs_ref
+def test_umat_vs_libcsf():
+    for nspin in range(0, 11):
+        for twoms in range(-(nspin % 2 + 0), nspin + 1, 2):
+            if twoms < 0 or (nspin - twoms) % 2:
+                continue
+            na = (nspin + twoms) // 2
+            nb = nspin - na
+            for smult in range(twoms + 1, nspin + 2, 2):
+                u = R.get_spin_evecs(nspin, na, nb, smult)
+                det = R.addrs2str(nspin, na, np.arange(u.shape[0]))
+                coup = R.gen_addrs2str(nspin, smult, np.arange(u.shape[1]))
+                ref = gasref.makecsf(det, coup, nspin, smult - 1, na - nb)
+                assert np.array_equal(u, ref)
+
+
+def test_c1_fixture_integer_maps():
+    import hashlib
+    g = load_golden("c1_norb12_6e6e_s0")
+    sha = lambda a: hashlib.sha256(np.ascontiguousarray(a, dtype="<u4").tobytes()).hexdigest()
+    csd = R.make_csd_mask(12, 6, 6)
+    assert sha(csd) == str(g["sha_csd_mask"])
+    assert np.array_equal(R.link_table(12, 6), g["link_a"])
