@@ -1,0 +1,329 @@
+"""Benchmark: CAS(16,16) singlet FP64 sigma throughput on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one sigma = sum_{pq,rs} h2e[pq,rs] E_pq E_rs c over the full
+CAS(16,16) (8,8) determinant space (165,636,900 determinants, 1.33 GB per
+vector), c a singlet vector produced from random CSFs (exactly what the
+Davidson loop of the CSF solver feeds to sigma).  Integrals: seeded
+synthetic h1/eri of rank 32 (no molecular data available offline).
+
+Our arm: ``value`` = sigma/s with c resident in HBM (inputs 1.33 GB >> the
+126 MB L2, so every step streams from HBM; no flush needed); ``e2e`` = the
+same through the public API (FCISolver.contract_2e on a pinned host vector,
+host->device copy of c and device->host copy of sigma inside the timed
+region).  ``roofline`` reports the sigma kernel against HBM with the
+algorithmic bytes 8*ndet*2*(nlink_a+nlink_b) per launch.  N>1: independent
+replicas, one per GPU (the path does not shard); value is the sum.
+
+Reference arm: the reference's own CPU sigma (pyscf/lib/mcscf GAS library
+with one subspace, built into oracle/_ref) on all host cores.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NORB, NELEC, RANK = 16, (8, 8), 32
+WORKLOAD = "CAS(16,16) (8,8) singlet FP64 sigma"
+METRIC = "CAS(16,16) FP64 sigma/s"
+
+
+def seeded_integrals(norb, rank, seed=0):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    h1 = rng.normal(0.0, 0.3, (norb, norb))
+    h1 = 0.5 * (h1 + h1.T)
+    np.fill_diagonal(h1, np.linspace(-2.0, 0.5, norb))
+    L = rng.normal(0.0, 0.2, (rank, norb * norb)).reshape(rank, norb, norb)
+    L = 0.5 * (L + L.transpose(0, 2, 1))
+    eri = 0.5 * np.einsum("xpq,xrs->pqrs", L, L)
+    return h1, eri
+
+
+def algorithmic(norb, nelec):
+    from math import comb
+    na, nb = nelec
+    ndet = comb(norb, na) * comb(norb, nb)
+    nla = na * (norb - na + 1)
+    nlb = nb * (norb - nb + 1)
+    npair = norb * (norb + 1) // 2
+    return ndet, 8.0 * ndet * 2 * (nla + nlb), 2.0 * ndet * npair ** 2
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        import statistics
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_sigma(norb, nelec, rank, budget_s=25.0, min_steps=1):
+    """Time the reference's own CPU sigma (fci_contract_gas_plan_execute,
+    pyscf/lib/mcscf/fci_contract_gas.c:2423) on all host threads.  Returns
+    (sigma/s, cores, sample description)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import gasref
+    import restate as R
+    cores = len(os.sched_getaffinity(0))
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    from math import comb
+    cpu_model = ""
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                cpu_model = ln.split(":", 1)[1].strip()
+                break
+    except Exception:
+        pass
+
+    def timed(no, ne, rk, budget, nmin):
+        h1, eri = seeded_integrals(no, rk)
+        h2e = R.absorb_h1e(h1, eri, no, ne, 0.5)
+        plan = gasref.SigmaPlan(no, ne, h2e)
+        nd = comb(no, ne[0]) * comb(no, ne[1])
+        ci = np.random.default_rng(1).normal(size=nd)
+        ci /= np.linalg.norm(ci)
+        n = 0
+        t0 = time.perf_counter()
+        while True:
+            plan(ci)
+            n += 1
+            el = time.perf_counter() - t0
+            if n >= nmin and (el > budget / 2 or el + el / n > budget):
+                break
+        plan.close()
+        return n, el
+
+    # a CAS(14,14) sigma first; run the full CAS(16,16) sigma when the host
+    # finishes it within the budget, else scale by the flop ratio
+    n14, t14 = timed(14, (7, 7), 28, min(budget_s, 10.0), 1)
+    ratio = algorithmic(norb, nelec)[2] / algorithmic(14, (7, 7))[2]
+    est = t14 / n14 * ratio
+    if est <= budget_s:
+        n, el = timed(norb, nelec, rank, budget_s, min_steps)
+        return n / el, cores, "%d full CAS(%d,%d) sigma(s) in %.1f s on %d threads (%s)" % (
+            n, norb, norb, el, cores, cpu_model)
+    return (n14 / t14) / ratio, cores, (
+        "%d CAS(14,14) (7,7) sigma(s) in %.1f s on %d threads (%s), scaled to CAS(16,16) by the "
+        "flop ratio %.1f (a full CAS(16,16) sigma is estimated at %.0f s here)" % (
+            n14, t14, cores, cpu_model, ratio, est))
+
+
+def run_reference(args, rank_env):
+    rank, world = rank_env
+    if rank != 0:
+        return
+    value, cores, sample = cpu_reference_sigma(NORB, NELEC, RANK, budget_s=max(30.0, 20.0 * args.steps / 10),
+                                               min_steps=1)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "sigma/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "norb": NORB, "nelec": list(NELEC), "eri_rank": RANK},
+            "cpu_baseline": {"value": value, "unit": "sigma/s", "cores": cores, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "sigma/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank_env):
+    import numpy as np
+    import torch
+    rank, world = rank_env
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    import pyscf_forge_b200 as P
+    from pyscf_forge_b200 import _capi
+    from pyscf_forge_b200.fci import direct_spin1 as D
+    from pyscf_forge_b200.csf_fci.csfstring import CSFTransformer
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+    h1, eri = seeded_integrals(NORB, RANK)
+    sol = P.csf_solver(None, smult=1)
+    sol.norb, sol.nelec = NORB, NELEC
+    sol.check_transformer_cache()
+    t = sol.transformer
+    h2eff = sol.absorb_h1e(h1, eri, NORB, NELEC, 0.5)
+    g = torch.Generator(device="cpu").manual_seed(1 + rank)
+    x = torch.randn(t.ncsf, generator=g, dtype=torch.float64).cuda()
+    c = t.dev_csf2det(x)[0]
+    c /= torch.linalg.norm(c)
+    eta = t.spin_parity
+    del x
+    out = torch.empty_like(c)
+    ndet, B, F = algorithmic(NORB, NELEC)
+
+    def step():
+        D.dev_contract_2e(h2eff.h2e, c, NORB, NELEC, eta=eta, out=out)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    _capi.profile_enable(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        barrier()
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        barrier()
+    prof = _capi.profile_report()
+    _capi.profile_enable(False)
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        tt = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * 1000.0 / ms
+    k_cnt, k_ms = prof.get("k_sigma", (0, 0.0))
+    k_avg_ms = k_ms / max(k_cnt, 1)
+    launches = sum(v[0] for v in prof.values())
+
+    # end-to-end through the public API: pinned host vector in, host sigma out
+    ch = torch.empty(ndet, dtype=torch.float64).pin_memory()
+    ch.copy_(c.cpu())  # contract_2e detects the singlet symmetry of ch on the device
+    e2e_steps = max(1, min(args.steps, 3))
+    sol.contract_2e(h2eff, ch, NORB, NELEC)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        res = sol.contract_2e(h2eff, ch, NORB, NELEC)
+    barrier()
+    e2e_ms = (time.perf_counter() - t0) * 1000.0 / e2e_steps
+    if world > 1:
+        tt = torch.tensor([e2e_ms], device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    # the public-API result must equal the device step
+    step()
+    torch.cuda.synchronize()
+    err = float((res.to(out.device) - out).abs().max())
+    assert err < 1e-9, err
+
+    hbm, src = peaks()
+    achieved = B / (k_avg_ms * 1e-3) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": "sigma/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded rank-32 integrals, random singlet CSF vector)",
+            "config": {"workload": WORKLOAD, "norb": NORB, "nelec": list(NELEC), "eri_rank": RANK,
+                       "ndet": ndet, "l2": "inputs 1.33 GB >> 126 MB L2 (no flush needed)",
+                       "parallelism": "replicas%d" % world},
+            "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "sigma/s",
+                    "h2d_bytes_per_step": ndet * 8, "d2h_bytes_per_step": ndet * 8,
+                    "note": "FCISolver.contract_2e on a pinned host vector"},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None,
+                         "kernel": "k_sigma", "algorithmic_bytes": B,
+                         "flops": F, "tflops": F / (k_avg_ms * 1e-3) / 1e12,
+                         "peak_note": "hbm_gbs %s (MEASURED_PEAKS.json)" % src},
+            "clocks": clk.summary()}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, cores, sample = cpu_reference_sigma(NORB, NELEC, RANK, budget_s=20.0)
+        line["cpu_baseline"] = {"value": v, "unit": "sigma/s", "cores": cores, "kind": "reference",
+                                "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, (rank, world))
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, (rank, world))
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

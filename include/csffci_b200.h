@@ -71,6 +71,13 @@ typedef struct {
 int csffci_abi_version(void);
 const char* csffci_last_error(void);
 
+/* Per-kernel CUDA-event timing on the calling host thread (off by default).
+ * enable(1) clears previous records; report() synchronises the recorded
+ * events and writes "kernel count total_ms" lines into buf.  No counterpart
+ * in the reference (its timing is logger checkpoints, csf.py:387-491). */
+int csffci_profile_enable(int on);
+int csffci_profile_report(char* buf, size_t len);
+
 /* ---- strings and link tables (PySCF cistring; reference twin
  *      pyscf/lib/mcscf/fci_string_gas.c:263-298, 1304-1427) ------------- */
 
@@ -156,6 +163,11 @@ enum {
 };
 
 size_t csffci_sigma_workspace(int norb, int neleca, int nelecb, int flags);
+/* out3 = (max|c - c^T|, max|c + c^T|, max|c|) of a square n x n CI matrix
+ * (device); decides whether CSFFCI_SIGMA_SPIN_SYMMETRIC applies.  work:
+ * 148*4*3 doubles.  No counterpart in the reference. */
+int csffci_spin_parity(int64_t n, const double* c, double* out3, void* work,
+                       size_t work_bytes, cudaStream_t stream);
 /* sigma = sum_{pq,rs} h2e[pq][rs] E_pq E_rs ci.  eta (+1/-1) is used only
  * with CSFFCI_SIGMA_SPIN_SYMMETRIC. */
 int csffci_sigma(int norb, int neleca, int nelecb, const double* h2e,

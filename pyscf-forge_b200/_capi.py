@@ -46,6 +46,8 @@ _p = ctypes.c_void_p
 _SIGS = {
     "csffci_abi_version": ([], _i),
     "csffci_last_error": ([], ctypes.c_char_p),
+    "csffci_profile_enable": ([_i], _i),
+    "csffci_profile_report": ([ctypes.c_char_p, _sz], _i),
     "csffci_gen_strings": ([_i, _i, _p, _p], _i),
     "csffci_link_table": ([_i, _i, _p, _p], _i),
     "csffci_csd_masks": ([_i, _i, _i, _i, _p, _p, _p, _p], _i),
@@ -59,6 +61,7 @@ _SIGS = {
     "csffci_hdiag_csf": ([_i, _i, _i, _p, _p, _p, _p, _i, _p, _p], _i),
     "csffci_pspace_h0": ([_i, _i, _i, _p, _p, _p, _p, _p, _i, _p, _p], _i),
     "csffci_sigma_workspace": ([_i, _i, _i, _i], _sz),
+    "csffci_spin_parity": ([_i64, _p, _p, _p, _sz, _p], _i),
     "csffci_sigma": ([_i, _i, _i, _p, _p, _p, _p, _p, _i, _i, _p, _sz, _p], _i),
     "csffci_contract_1e": ([_i, _i, _i, _p, _p, _p, _p, _p, _p, _p], _i),
     "csffci_rdm12_workspace": ([_i, _i, _i], _sz),
@@ -120,3 +123,18 @@ def call(name, *args):
 
 def query(name, *args):
     return getattr(load(), name)(*args)
+
+
+def profile_enable(on=True):
+    call("csffci_profile_enable", 1 if on else 0)
+
+
+def profile_report():
+    """{kernel: (launches, total_ms)} recorded since profile_enable(True)."""
+    buf = ctypes.create_string_buffer(1 << 16)
+    call("csffci_profile_report", buf, len(buf))
+    out = {}
+    for line in buf.value.decode().splitlines():
+        name, cnt, ms = line.split()
+        out[name] = (int(cnt), float(ms))
+    return out

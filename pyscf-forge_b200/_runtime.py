@@ -63,7 +63,7 @@ def to_dev(x, dtype=torch.float64):
 def like_input(result, ref):
     """Return a torch tensor if the caller passed torch, else numpy."""
     if isinstance(ref, torch.Tensor):
-        return result
+        return result.to(ref.device)
     return result.detach().cpu().numpy()
 
 

@@ -15,7 +15,7 @@ import numpy as np
 import torch
 
 from .. import _capi
-from .._runtime import device, eri_pair_matrix, ptr, require_cuda, stream, to_dev
+from .._runtime import device, eri_pair_matrix, like_input, ptr, require_cuda, stream, to_dev
 from ..fci import direct_spin1
 from ..fci.davidson import DiagPrecond, davidson, gram
 from ..fci.direct_spin1 import _unpack_nelec
@@ -383,11 +383,14 @@ class CSFFCISolver:
         else:
             h2e, h1e_s = to_dev(eri_pair_matrix(eri, norb)), None
         ci = to_dev(fcivec).reshape(-1)
-        hc = direct_spin1.dev_contract_2e(h2e, ci, norb, nelec)
+        eta = None
+        if nelec[0] == nelec[1]:
+            eta = direct_spin1.dev_spin_parity(ci, comb(norb, nelec[0]))
+        hc = direct_spin1.dev_contract_2e(h2e, ci, norb, nelec, eta=eta)
         if h1e_s is not None:
             direct_spin1.dev_contract_1e(h1e_s, -h1e_s, ci, norb, nelec, hc)
-        hc = hc.reshape(to_dev(fcivec).shape)
-        return hc if isinstance(fcivec, torch.Tensor) else hc.cpu().numpy()
+        shape = fcivec.shape if hasattr(fcivec, "shape") else np.shape(fcivec)
+        return like_input(hc.reshape(shape), fcivec)
 
     def pspace(self, h1e, eri, norb, nelec, hdiag_det=None, hdiag_csf=None, npsp=200, **kwargs):
         self.norb = norb

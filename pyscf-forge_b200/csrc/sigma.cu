@@ -14,6 +14,7 @@
 // the beta scatter is done and sigma = s + eta s^T, which removes every
 // cross-row update.
 #include "common.cuh"
+#include "profile.cuh"
 
 namespace csffci {
 
@@ -170,6 +171,53 @@ __global__ void k_sym_add(const double* __restrict__ s, double* out, long long n
   }
 }
 
+// per-block maxima of |c - c^T|, |c + c^T|, |c| over a square n x n matrix
+__global__ void k_parity_part(const double* __restrict__ c, long long n, double* part) {
+  __shared__ double s0[256], s1[256], s2[256];
+  double a = 0.0, b = 0.0, m = 0.0;
+  long long tot = n * n;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
+       i += (long long)gridDim.x * blockDim.x) {
+    long long r = i / n, q = i - r * n;
+    if (q > r) continue;
+    double x = c[i], y = c[q * n + r];
+    a = fmax(a, fabs(x - y));
+    b = fmax(b, fabs(x + y));
+    m = fmax(m, fmax(fabs(x), fabs(y)));
+  }
+  s0[threadIdx.x] = a;
+  s1[threadIdx.x] = b;
+  s2[threadIdx.x] = m;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      s0[threadIdx.x] = fmax(s0[threadIdx.x], s0[threadIdx.x + w]);
+      s1[threadIdx.x] = fmax(s1[threadIdx.x], s1[threadIdx.x + w]);
+      s2[threadIdx.x] = fmax(s2[threadIdx.x], s2[threadIdx.x + w]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[3 * blockIdx.x] = s0[0];
+    part[3 * blockIdx.x + 1] = s1[0];
+    part[3 * blockIdx.x + 2] = s2[0];
+  }
+}
+
+__global__ void k_parity_final(const double* part, int np, double* out3) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double a = 0, b = 0, m = 0;
+    for (int i = 0; i < np; ++i) {
+      a = fmax(a, part[3 * i]);
+      b = fmax(b, part[3 * i + 1]);
+      m = fmax(m, part[3 * i + 2]);
+    }
+    out3[0] = a;
+    out3[1] = b;
+    out3[2] = m;
+  }
+}
+
 struct SigmaConfig {
   int npad, hstride, dstride, nt, threads;
   bool hsmem;
@@ -221,6 +269,7 @@ template <int NT, bool HS>
 static int launch_sigma(const SigmaConfig& c, SigmaArgs& g, int grid, cudaStream_t stream) {
   auto kern = k_sigma<NT, HS>;
   CSF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
+  ProfScope ps("k_sigma", stream);
   kern<<<grid, c.threads, c.smem, stream>>>(g);
   return check_launch("sigma");
 }
@@ -230,6 +279,22 @@ static int launch_sigma(const SigmaConfig& c, SigmaArgs& g, int grid, cudaStream
 using namespace csffci;
 
 extern "C" {
+
+int csffci_spin_parity(int64_t n, const double* c, double* out3, void* work, size_t work_bytes,
+                       cudaStream_t stream) {
+  CSF_REQUIRE(n >= 0 && out3 != nullptr, "spin_parity: bad arguments");
+  const int np = 148 * 4;
+  if (work == nullptr || work_bytes < (size_t)(3 * np) * sizeof(double)) {
+    set_error("spin_parity: workspace of %zu bytes < %zu required", work_bytes,
+              (size_t)(3 * np) * sizeof(double));
+    return CSFFCI_ERR_MEMORY;
+  }
+  k_parity_part<<<np, 256, 0, stream>>>(c, n, (double*)work);
+  int st = check_launch("spin_parity");
+  if (st) return st;
+  k_parity_final<<<1, 32, 0, stream>>>((double*)work, np, out3);
+  return check_launch("spin_parity final");
+}
 
 size_t csffci_sigma_workspace(int norb, int neleca, int nelecb, int flags) {
   if (flags & CSFFCI_SIGMA_SPIN_SYMMETRIC)
@@ -307,6 +372,7 @@ int csffci_sigma(int norb, int neleca, int nelecb, const double* h2e, const csff
   if (st) return st;
   if (sym) {
     dim3 blk(32, 8);
+    ProfScope ps("k_sym_add", stream);
     long long tiles = ((Na + 31) / 32) * ((Na + 31) / 32);
     k_sym_add<<<grid_for(tiles, 1, 148 * 16), blk, 0, stream>>>(target, sigma, Na, (double)eta,
                                                                accumulate ? 1 : 0);

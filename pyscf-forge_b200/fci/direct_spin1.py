@@ -108,6 +108,22 @@ def dev_contract_2e(h2e, ci, norb, nelec, eta=None, out=None, accumulate=False):
     return out
 
 
+def dev_spin_parity(ci, n, rtol=1e-12):
+    """+1 / -1 if the (n, n) CI matrix is symmetric / antisymmetric to
+    rtol*max|c|, else None (decides the spin-symmetric sigma path)."""
+    out = torch.empty(3, dtype=torch.float64, device=ci.device)
+    ws = workspace("parity", 148 * 4 * 3 * 8)
+    _capi.call("csffci_spin_parity", n, ptr(ci), ptr(out), ptr(ws), ws.numel(), stream())
+    a, b, m = out.cpu().numpy()
+    if m == 0.0:
+        return None
+    if a <= rtol * m:
+        return 1
+    if b <= rtol * m:
+        return -1
+    return None
+
+
 def dev_contract_1e(h1a, h1b, ci, norb, nelec, out):
     """out += sum h1a[p,q] Ea_pq ci + h1b[p,q] Eb_pq ci (csf.py:527-528)."""
     na, nb = nelec
@@ -159,7 +175,8 @@ def contract_2e(eri, fcivec, norb, nelec, link_index=None):
     nelec = _unpack_nelec(nelec)
     h2e = to_dev(eri_pair_matrix(eri, norb))
     ci = to_dev(fcivec)
-    out = dev_contract_2e(h2e, ci.reshape(-1), norb, nelec)
+    eta = dev_spin_parity(ci, num_strings(norb, nelec[0])) if nelec[0] == nelec[1] else None
+    out = dev_contract_2e(h2e, ci.reshape(-1), norb, nelec, eta=eta)
     return like_input(out.reshape(ci.shape), fcivec)
 
 
