@@ -157,9 +157,11 @@ int csffci_pspace_h0(int norb, int neleca, int nelecb, const double* h1a,
 
 enum {
   CSFFCI_SIGMA_ACCUMULATE = 1, /* add into sigma instead of overwriting */
-  CSFFCI_SIGMA_SPIN_SYMMETRIC = 2 /* ci == eta * ci^T (na == nb): only the
-                                     row-local half is formed, then
-                                     sigma = s + eta * s^T */
+  CSFFCI_SIGMA_SPIN_SYMMETRIC = 2, /* ci == eta * ci^T (na == nb): only the
+                                      Jb <= Ja half of the contraction is
+                                      formed, then sigma = s + eta * s^T */
+  CSFFCI_SIGMA_REFERENCE_KERNEL = 4 /* force the simple shared-memory-h2e
+                                       kernel (used to cross-check) */
 };
 
 size_t csffci_sigma_workspace(int norb, int neleca, int nelecb, int flags);

@@ -15,6 +15,7 @@
 // cross-row update.
 #include "common.cuh"
 #include "profile.cuh"
+#include "sigma_rr.cuh"
 
 namespace csffci {
 
@@ -327,6 +328,19 @@ int csffci_sigma(int norb, int neleca, int nelecb, const double* h2e, const csff
   if (sym || !accumulate) CSF_CUDA(cudaMemsetAsync(target, 0, ndet * sizeof(double), stream));
   if (ndet == 0) return CSFFCI_OK;
 
+  if (sigma_rr_supported(norb) && !(flags & CSFFCI_SIGMA_REFERENCE_KERNEL)) {
+    int st = sigma_rr_run(norb, neleca, nelecb, h2e, link_a, link_b, ci, target, sym, (double)eta, stream);
+    if (st) return st;
+    if (sym) {
+      dim3 blk(32, 8);
+      ProfScope ps("k_sym_add", stream);
+      long long tiles = ((Na + 31) / 32) * ((Na + 31) / 32);
+      k_sym_add<<<grid_for(tiles, 1, 148 * 16), blk, 0, stream>>>(target, sigma, Na, (double)eta,
+                                                                 accumulate ? 1 : 0);
+      return check_launch("sigma symmetric add");
+    }
+    return CSFFCI_OK;
+  }
   SigmaConfig c = sigma_config(norb, nla);
   CSF_REQUIRE(c.nt > 0, "sigma: no tile configuration fits shared memory for norb=%d", norb);
   SigmaArgs g;

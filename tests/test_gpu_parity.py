@@ -342,3 +342,32 @@ def test_errors_are_raised():
     t = C.CSFTransformer(6, 3, 3, 1)
     with pytest.raises(C.ImpossibleCIvecError):
         t.vec_det2csf(np.zeros(17))
+
+
+@pytest.mark.parametrize("norb,nelec,smult", [(8, (4, 4), 1), (10, (5, 5), 3), (12, (6, 6), 1),
+                                              (11, (6, 5), 2), (9, (6, 2), 5), (14, (5, 5), 1)])
+def test_sigma_kernels_agree(norb, nelec, smult):
+    """The register-resident kernel (general and spin-symmetric modes)
+    against the simple shared-memory kernel and, where small enough, the
+    reference C."""
+    _, D, C = _mods()
+    from pyscf_forge_b200 import _capi
+    from pyscf_forge_b200._runtime import ptr, stream, workspace
+    h1, eri = seeded_integrals(norb, 10, seed=4)
+    h2e = D.dev_absorb_h1e(h1, R.restore4(eri, norb), norb, nelec, 0.5)
+    t = C.CSFTransformer(norb, nelec[0], nelec[1], smult)
+    g = torch.Generator(device="cpu").manual_seed(3)
+    c = t.dev_csf2det(torch.randn(t.ncsf, generator=g, dtype=torch.float64).cuda())[0]
+    la, lb = D.dev_link_table(norb, nelec[0]), D.dev_link_table(norb, nelec[1])
+    ref = torch.empty_like(c)
+    _capi.call("csffci_sigma", norb, nelec[0], nelec[1], ptr(h2e), ptr(la), ptr(lb), ptr(c), ptr(ref),
+               _capi.SIGMA_REFERENCE_KERNEL, 1, None, 0, stream())
+    got = D.dev_contract_2e(h2e, c, norb, nelec)
+    torch.testing.assert_close(got, ref, atol=1e-11, rtol=0)
+    if t.spin_parity is not None:
+        got2 = D.dev_contract_2e(h2e, c, norb, nelec, eta=t.spin_parity)
+        torch.testing.assert_close(got2, ref, atol=1e-11, rtol=0)
+    if gasref.available() and c.numel() < 2e6:
+        h2e_np = h2e.cpu().numpy()
+        np.testing.assert_allclose(got.cpu().numpy(), gasref.contract_2e(h2e_np, c.cpu().numpy(), norb, nelec),
+                                   atol=1e-10)
