@@ -137,6 +137,23 @@ int csffci_hdiag_det(int norb, int neleca, int nelecb, const double* h1a,
                      const double* h1b, const double* eri, double* hdiag,
                      void* work, size_t work_bytes, cudaStream_t stream);
 
+/* Same result as csffci_hdiag_det, but allocates nothing and takes no
+ * workspace: for callers that cannot call cudaMalloc (device memory owned by
+ * another allocator with a fixed budget, or loops where an allocation would
+ * synchronise the device) and so have no buffer to lend.  No counterpart in
+ * the reference.  Its scratch is a fixed array of
+ * CSFFCI_HDIAG_NOALLOC_MAX_DOUBLES doubles (2 MiB) inside the library,
+ * held by every GPU that loads it until exit; spaces needing more
+ * (Na*(norb+1) + 2*Nb doubles; up to norb = 16 at half filling fits) are
+ * rejected with CSFFCI_ERR_MEMORY.  The first call on a device looks up
+ * the array's device address, so make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other
+ * streams, other host threads) race and must be serialised by the caller. */
+#define CSFFCI_HDIAG_NOALLOC_MAX_DOUBLES (1 << 18)
+int csffci_hdiag_det_noalloc(int norb, int neleca, int nelecb, const double* h1a,
+                             const double* h1b, const double* eri, double* hdiag,
+                             cudaStream_t stream);
+
 /* CSF diagonal computed per configuration on the fly (make_hdiag_csf,
  * csf.py:70-144, which materialises (nconf,ndet,ndet) blocks instead).
  * blocks[i].zmat must be set (csffci_spin_exchange_table). */

@@ -59,6 +59,7 @@ _SIGS = {
     "csffci_absorb_h1e": ([_i, _i, _p, _p, _d, _p, _p], _i),
     "csffci_hdiag_det_workspace": ([_i, _i, _i], _sz),
     "csffci_hdiag_det": ([_i, _i, _i, _p, _p, _p, _p, _p, _sz, _p], _i),
+    "csffci_hdiag_det_noalloc": ([_i, _i, _i, _p, _p, _p, _p, _p], _i),
     "csffci_hdiag_csf": ([_i, _i, _i, _p, _p, _p, _p, _i, _p, _p], _i),
     "csffci_pspace_h0": ([_i, _i, _i, _p, _p, _p, _p, _p, _i, _p, _p], _i),
     "csffci_sigma_workspace": ([_i, _i, _i, _i], _sz),

@@ -1,5 +1,7 @@
 // Hamiltonian building blocks: absorb_h1e, the determinant diagonal, the
 // p-space Slater-Condon block and the one-electron contraction.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace csffci {
@@ -275,3 +277,83 @@ int csffci_contract_1e(int norb, int neleca, int nelecb, const double* h1a, cons
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Determinant diagonal without any allocation and without a caller
+// workspace.
+//
+// Some callers cannot call cudaMalloc: a host program whose device memory
+// is owned entirely by another allocator (a framework's caching pool with a
+// fixed budget, where a raw cudaMalloc would grow memory behind its back),
+// or a latency-sensitive loop where cudaMalloc/cudaFree would synchronise
+// the device.  Such callers also have no spare buffer to hand over as the
+// workspace that csffci_hdiag_det needs.  This variant keeps that
+// workspace in a fixed array that is part of the library image instead.
+//
+// The array below is CSFFCI_HDIAG_NOALLOC_MAX_DOUBLES doubles (2 MiB).  Every
+// GPU that loads the library holds it until the process exits.  It fits the
+// per-string tables of up to norb = 16 at half filling: Na*(norb+1) + Nb
+// doubles plus Nb 64-bit strings.  Larger spaces are rejected.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double g_hdiag_noalloc_scratch[CSFFCI_HDIAG_NOALLOC_MAX_DOUBLES];
+
+namespace csffci {
+namespace {
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[256] = {nullptr};  // device address of the array, per device ordinal
+}  // namespace
+}  // namespace csffci
+
+extern "C" int csffci_hdiag_det_noalloc(int norb, int neleca, int nelecb, const double* h1a,
+                                        const double* h1b, const double* eri, double* hdiag,
+                                        cudaStream_t stream) {
+  CSF_REQUIRE(norb >= 1 && norb <= 63 && neleca >= 0 && nelecb >= 0 && neleca <= norb &&
+                  nelecb <= norb,
+              "hdiag_det_noalloc: bad (norb=%d, nelec=(%d,%d))", norb, neleca, nelecb);
+  const unsigned long long Na = host_binom(norb, neleca), Nb = host_binom(norb, nelecb);
+  const unsigned long long need = Na * (unsigned long long)(norb + 1) + 2ull * Nb;
+  if (need > (unsigned long long)CSFFCI_HDIAG_NOALLOC_MAX_DOUBLES) {
+    set_error("hdiag_det_noalloc: (norb=%d, nelec=(%d,%d)) needs %llu doubles of scratch, more "
+              "than the fixed %d; use csffci_hdiag_det with a workspace",
+              norb, neleca, nelecb, need, CSFFCI_HDIAG_NOALLOC_MAX_DOUBLES);
+    return CSFFCI_ERR_MEMORY;
+  }
+  // The symbol's name is a host-side stand-in, not a device address: look
+  // the address up once per device, with that device current.
+  int dev = 0;
+  CSF_CUDA(cudaGetDevice(&dev));
+  CSF_REQUIRE(dev >= 0 && dev < 256, "hdiag_det_noalloc: device ordinal %d out of range", dev);
+  void* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_ptr[dev] == nullptr) {
+      void* p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_hdiag_noalloc_scratch);
+      if (e != cudaSuccess || p == nullptr) {
+        set_error("hdiag_det_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev,
+                  cudaGetErrorString(e));
+        return CSFFCI_ERR_CUDA;
+      }
+      g_noalloc_ptr[dev] = p;
+    }
+    base = g_noalloc_ptr[dev];
+  }
+  // Every entry of the scratch that the kernels read is written first by the
+  // same call (ea, ja, eb and the beta strings), so nothing needs clearing.
+  const int npair = norb * (norb + 1) / 2;
+  double* ea = (double*)base;
+  double* ja = ea + Na;
+  double* eb = ja + Na * norb;
+  uint64_t* sb = (uint64_t*)(eb + Nb);
+  k_string_energy<<<grid_for((long long)Na, 128), 128, 0, stream>>>(norb, neleca, npair, Na, h1a,
+                                                                    eri, ea, ja, nullptr);
+  int st = check_launch("hdiag_det_noalloc alpha strings");
+  if (st) return st;
+  k_string_energy<<<grid_for((long long)Nb, 128), 128, 0, stream>>>(norb, nelecb, npair, Nb, h1b,
+                                                                    eri, eb, nullptr, sb);
+  st = check_launch("hdiag_det_noalloc beta strings");
+  if (st) return st;
+  k_hdiag_det<<<grid_for((long long)(Na * Nb), 256, 148 * 32), 256, 0, stream>>>(norb, Na, Nb, ea,
+                                                                                  eb, ja, sb, hdiag);
+  return check_launch("hdiag_det_noalloc");
+}
