@@ -33,6 +33,13 @@ sys.path.insert(0, ROOT)
 NORB, NELEC, RANK = 16, (8, 8), 32
 WORKLOAD = "CAS(16,16) (8,8) singlet FP64 sigma"
 METRIC = "CAS(16,16) FP64 sigma/s"
+# smaller singlet cases of the same kernel, for profiling captures
+WORKLOADS = {"cas16": (16, (8, 8), 32), "cas14": (14, (7, 7), 28), "cas12": (12, (6, 6), 24)}
+
+
+# DRAM bytes (read + write) per k_sigma_rr launch from ncu (profiles/); None
+# until captured for the current kernel
+TRAFFIC = {}
 
 
 def seeded_integrals(norb, rank, seed=0):
@@ -203,6 +210,7 @@ def run_ours(args, rank_env):
     from pyscf_forge_b200.csf_fci.csfstring import CSFTransformer
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
+    NORB, NELEC, RANK = WORKLOADS[args.workload]
     h1, eri = seeded_integrals(NORB, RANK)
     sol = P.csf_solver(None, smult=1)
     sol.norb, sol.nelec = NORB, NELEC
@@ -217,6 +225,7 @@ def run_ours(args, rank_env):
     del x
     out = torch.empty_like(c)
     ndet, B, F = algorithmic(NORB, NELEC)
+    traffic = TRAFFIC.get(args.workload)
 
     def step():
         D.dev_contract_2e(h2eff.h2e, c, NORB, NELEC, eta=eta, out=out)
@@ -247,10 +256,13 @@ def run_ours(args, rank_env):
         torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
         ms = float(tt.item())
     value = world * 1000.0 / ms
-    k_cnt, k_ms = prof.get("k_sigma", (0, 0.0))
+    k_cnt, k_ms = prof.get("k_sigma_rr", prof.get("k_sigma", (0, 0.0)))
     k_avg_ms = k_ms / max(k_cnt, 1)
     launches = sum(v[0] for v in prof.values())
 
+    if args.no_e2e:
+        print(json.dumps({"workload": args.workload, "ms_per_step": ms, "kernel_ms": k_avg_ms}), flush=True)
+        return
     # end-to-end through the public API: pinned host vector in, host sigma out
     ch = torch.empty(ndet, dtype=torch.float64).pin_memory()
     ch.copy_(c.cpu())  # contract_2e detects the singlet symmetry of ch on the device
@@ -274,6 +286,7 @@ def run_ours(args, rank_env):
 
     hbm, src = peaks()
     achieved = B / (k_avg_ms * 1e-3) / 1e9
+    dmma = _capi.fp64_peak(0)
     line = {"metric": METRIC, "value": value, "unit": "sigma/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -286,9 +299,14 @@ def run_ours(args, rank_env):
                     "note": "FCISolver.contract_2e on a pinned host vector"},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None,
-                         "kernel": "k_sigma", "algorithmic_bytes": B,
+                         "frac": achieved / hbm, "traffic": traffic,
+                         "kernel": "k_sigma_rr" if "k_sigma_rr" in prof else "k_sigma",
+                         "algorithmic_bytes": B,
                          "flops": F, "tflops": F / (k_avg_ms * 1e-3) / 1e12,
+                         "flops_formed": F / 2, "dmma_peak_tflops": dmma,
+                         "frac_dmma": (F / 2) / (k_avg_ms * 1e-3) / 1e12 / dmma,
+                         "dmma_note": "singlet lower triangle forms F/2; DMMA peak measured live "
+                                      "(register-only m8n8k4 loop, csffci_fp64_peak)",
                          "peak_note": "hbm_gbs %s (MEASURED_PEAKS.json)" % src},
             "clocks": clk.summary()}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -306,6 +324,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="cas16", choices=sorted(WORKLOADS),
+                    help="cas16 is the benchmark; the smaller ones exist for profiling captures")
+    ap.add_argument("--no-e2e", action="store_true", help="time the device loop only (profiling)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

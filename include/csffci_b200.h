@@ -77,6 +77,11 @@ const char* csffci_last_error(void);
  * in the reference (its timing is logger checkpoints, csf.py:387-491). */
 int csffci_profile_enable(int on);
 int csffci_profile_report(char* buf, size_t len);
+/* FP64 throughput of a register-only loop on the current device (kind 0:
+ * DMMA m8n8k4, kind 1: DFMA), in TFLOP/s; synchronises the stream.  The
+ * FP64 roofline denominator for the sigma kernel.  No counterpart in the
+ * reference. */
+int csffci_fp64_peak(int kind, int iters, double* tflops, cudaStream_t stream);
 
 /* ---- strings and link tables (PySCF cistring; reference twin
  *      pyscf/lib/mcscf/fci_string_gas.c:263-298, 1304-1427) ------------- */

@@ -49,6 +49,7 @@ _SIGS = {
     "csffci_last_error": ([], ctypes.c_char_p),
     "csffci_profile_enable": ([_i], _i),
     "csffci_profile_report": ([ctypes.c_char_p, _sz], _i),
+    "csffci_fp64_peak": ([_i, _i, ctypes.POINTER(_d), _p], _i),
     "csffci_gen_strings": ([_i, _i, _p, _p], _i),
     "csffci_link_table": ([_i, _i, _p, _p], _i),
     "csffci_csd_masks": ([_i, _i, _i, _i, _p, _p, _p, _p], _i),
@@ -140,3 +141,10 @@ def profile_report():
         name, cnt, ms = line.split()
         out[name] = (int(cnt), float(ms))
     return out
+
+
+def fp64_peak(kind=0, iters=20000, stream=None):
+    """Measured FP64 TFLOP/s (kind 0: DMMA, 1: DFMA) on the current device."""
+    out = ctypes.c_double(0.0)
+    call("csffci_fp64_peak", int(kind), int(iters), ctypes.byref(out), stream)
+    return out.value

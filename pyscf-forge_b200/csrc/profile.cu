@@ -37,6 +37,39 @@ ProfScope::~ProfScope() {
   prof_record(name_, a_, b_);
 }
 
+// Register-only FP64 throughput loops (DMMA m8n8k4 and DFMA), used to
+// measure the FP64 roofline denominator on the running GPU.
+__global__ void k_peak_dmma(double* sink, int iters) {
+  double c[8][2];
+  for (int t = 0; t < 8; ++t) c[t][0] = c[t][1] = 0.0;
+  const double a = 1e-3 * threadIdx.x, b = 1e-3 * blockIdx.x;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                   : "+d"(c[t][0]), "+d"(c[t][1])
+                   : "d"(a), "d"(b));
+  }
+  double s = 0.0;
+  for (int t = 0; t < 8; ++t) s += c[t][0] + c[t][1];
+  if (s == 1234.5678) sink[0] = s;
+}
+
+__global__ void k_peak_dfma(double* sink, int iters) {
+  double c[8];
+  for (int t = 0; t < 8; ++t) c[t] = threadIdx.x * 1e-3 + t;
+  const double a = 1.0000001, b = 1e-9;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int t = 0; t < 8; ++t) c[t] = fma(c[t], a, b);
+  }
+  double s = 0.0;
+  for (int t = 0; t < 8; ++t) s += c[t];
+  if (s == 1234.5678) sink[0] = s;
+}
+
+static __device__ double g_peak_sink[1];
+
 }  // namespace csffci
 
 using namespace csffci;
@@ -52,6 +85,35 @@ int csffci_profile_enable(int on) {
   g_prof.ev.clear();
   g_prof.on = on != 0;
   return CSFFCI_OK;
+}
+
+int csffci_fp64_peak(int kind, int iters, double* tflops, cudaStream_t stream) {
+  CSF_REQUIRE(tflops != nullptr && iters > 0 && (kind == 0 || kind == 1), "fp64_peak: bad arguments");
+  int dev = 0, nsm = 148;
+  CSF_CUDA(cudaGetDevice(&dev));
+  CSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  double* sink = nullptr;
+  CSF_CUDA(cudaGetSymbolAddress((void**)&sink, g_peak_sink));
+  cudaEvent_t a, b;
+  CSF_CUDA(cudaEventCreate(&a));
+  CSF_CUDA(cudaEventCreate(&b));
+  const int blocks = nsm * 2, threads = 256;
+  if (kind == 0) k_peak_dmma<<<blocks, threads, 0, stream>>>(sink, 64);
+  else k_peak_dfma<<<blocks, threads, 0, stream>>>(sink, 64);
+  cudaEventRecord(a, stream);
+  if (kind == 0) k_peak_dmma<<<blocks, threads, 0, stream>>>(sink, iters);
+  else k_peak_dfma<<<blocks, threads, 0, stream>>>(sink, iters);
+  cudaEventRecord(b, stream);
+  CSF_CUDA(cudaEventSynchronize(b));
+  float ms = 0.f;
+  CSF_CUDA(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  const double warps = (double)blocks * threads / 32.0;
+  const double flops = kind == 0 ? 2.0 * 8 * 8 * 4 * 8 * (double)iters * warps
+                                 : 2.0 * 8 * (double)iters * blocks * threads;
+  *tflops = flops / (ms * 1e-3) / 1e12;
+  return check_launch("fp64_peak");
 }
 
 int csffci_profile_report(char* buf, size_t len) {
