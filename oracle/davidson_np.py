@@ -75,7 +75,7 @@ def davidson(aop, x0, precond, tol=1e-10, max_cycle=100, max_space=12, lindep=1e
         h = 0.5 * (h + h.T)
         w, c = np.linalg.eigh(h)
         k = min(nroots, len(w))
-        if follow_state and x_prev is not None:
+        if follow_state and x_prev is not None and any(conv):
             ov = np.abs((np.array(x_prev) @ Vm.T) @ c)
             idx = []
             for i in range(len(x_prev)):

@@ -233,7 +233,8 @@ def kernel(fci, h1e, eri, norb, nelec, smult=None, idx_sym=None, ci0=None, tol=N
         pw = pv = None
 
     if pspace_size >= ncsf_sym and not davidson_only:
-        # csf.py:416-429: the p-space is the whole space
+        # csf.py:416-429: the p-space is the whole space (exact diagonalisation)
+        fci.converged = [True] * nroots if nroots > 1 else True
         if ncsf_sym == 1:
             civec = transformer.dev_csf2det(torch.as_tensor(pv[:, 0].reshape(1, 1), device=device()))
             return pw[0] + ecore, civec.reshape(na, nb)

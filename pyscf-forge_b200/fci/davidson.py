@@ -112,6 +112,8 @@ def davidson(aop, x0, precond, tol=1e-10, max_cycle=100, max_space=12, lindep=1e
     conv = [False] * nroots
     e = None
     new = x0.clone()
+    nrm = np.sqrt(np.maximum(np.diag(gram(new, new).cpu().numpy()), 1e-300))
+    new = new / torch.as_tensor(nrm, device=dev)[:, None]
     for icyc in range(max_cycle):
         # orthonormalise the new block against V and among itself
         added = []
@@ -135,7 +137,10 @@ def davidson(aop, x0, precond, tol=1e-10, max_cycle=100, max_space=12, lindep=1e
         h[k0:m, :m] = blk.T
         w, c = np.linalg.eigh(h[:m, :m])
         k = min(nroots, m)
-        if follow_state and x_prev is not None:
+        # follow roots by overlap only once some root has converged; before
+        # that the lowest Ritz values are taken (a poor early guess would
+        # otherwise lock a root onto a high-lying state)
+        if follow_state and x_prev is not None and any(conv):
             ov = np.abs(x_prev[:, :m] @ c)
             idx = []
             for i in range(ov.shape[0]):
@@ -165,7 +170,10 @@ def davidson(aop, x0, precond, tol=1e-10, max_cycle=100, max_space=12, lindep=1e
         for i in range(k):
             if conv[i]:
                 continue
-            ts.append(precond(R[i], e[i], X[i]).reshape(1, -1))
+            t = precond(R[i], e[i], X[i]).reshape(1, -1)
+            nt = float(np.sqrt(max(gram(t, t).cpu().numpy()[0, 0], 0.0)))
+            if nt > 0.0:
+                ts.append(t / nt)
         new = torch.cat(ts) if ts else X[:0]
         if m + new.shape[0] > space:
             # restart from the Ritz vectors (orthonormal, h diagonal)
