@@ -199,6 +199,34 @@ int csffci_sigma(int norb, int neleca, int nelecb, const double* h2e,
                  const double* ci, double* sigma, int flags, int eta, void* work,
                  size_t work_bytes, cudaStream_t stream);
 
+/* One sigma of a batch (csffci_sigma_batch).  The caller fills the first
+ * block; the library fills the rest.  sym = 1 asserts neleca == nelecb and
+ * ci = eta ci^T (the spin-symmetric kernel) and needs scratch (ndet
+ * doubles); otherwise scratch may be NULL. */
+typedef struct {
+  const double* h2e;
+  const csffci_link_t* link_a;
+  const csffci_link_t* link_b;
+  const double* ci;
+  double* sigma;
+  double* scratch;
+  int32_t neleca, nelecb, sym, eta;
+  /* filled by the library */
+  int64_t Na, Nb, unit_begin, nunits, tile_begin, elem_begin;
+  int32_t nla, nlb;
+} csffci_sigma_job_t;
+
+/* Many sigmas of one orbital count in one persistent launch (role of
+ * csf.py:449 applied to every vector of every problem of a batch; no
+ * counterpart in the reference, which solves one problem at a time).  Jobs
+ * may differ in h2e, electron numbers, spin mode and vectors.  jobs is a
+ * host array (updated in place with the bookkeeping fields); work holds the
+ * device copy of the job table: csffci_sigma_batch_workspace(njobs)
+ * bytes.  Every sigma is overwritten. */
+size_t csffci_sigma_batch_workspace(int njobs);
+int csffci_sigma_batch(int norb, int njobs, csffci_sigma_job_t* jobs, void* work,
+                       size_t work_bytes, cudaStream_t stream);
+
 /* sigma += sum_pq h1a[p,q] Ea_pq ci + h1b[p,q] Eb_pq ci (direct_uhf.contract_1e
  * as used for the spin part of h1e at csf.py:527-528). */
 int csffci_contract_1e(int norb, int neleca, int nelecb, const double* h1a,
@@ -248,6 +276,82 @@ int csffci_precond(int64_t n, const double* r, const double* x, const double* hd
 int csffci_precond_dots(int64_t n, const double* r, const double* x, const double* hdiag,
                         double e, double shift, double* out2, double* work,
                         cudaStream_t stream);
+
+/* ---- batched forms for many independent problems (no counterpart in the
+ *      reference, which solves one problem at a time; used by the lockstep
+ *      batched solver).  Descriptor arrays are host arrays; the library
+ *      fills their bookkeeping fields, copies them into work and launches
+ *      one kernel per call. ------------------------------------------------ */
+
+/* one npair block of one problem's transform over nvec vectors */
+typedef struct {
+  const double* x;
+  double* y;
+  const uint32_t* mask;
+  const double* umat;
+  int64_t ldx, ldy, csd_offset, csf_offset, nconf;
+  int32_t ndet, ncsf, nvec, pad;
+  double sign;
+  int64_t tile_begin; /* filled by the library */
+} csffci_transform_job_t;
+
+/* nvec rows of n determinants (leading dimension ld) to zero before a
+ * reverse (CSF -> det) transform */
+typedef struct {
+  double* y;
+  int64_t ld, n, nvec;
+  int64_t elem_begin; /* filled by the library */
+} csffci_zero_job_t;
+
+/* reverse = 0: det -> CSF; 1: CSF -> det (zero jobs run first).  work:
+ * njobs*sizeof(csffci_transform_job_t) + nzero*sizeof(csffci_zero_job_t). */
+int csffci_transform_batch(int reverse, int njobs, csffci_transform_job_t* jobs, int nzero,
+                           csffci_zero_job_t* zjobs, void* work, size_t work_bytes,
+                           cudaStream_t stream);
+
+/* out[out_index] = sum_k x[k] y[k] (* P[k] when hdiag != NULL, P = the
+ * capped 1/(hdiag - e_shift)); one block per dot, fixed-order reduction.
+ * work: ndots*sizeof(csffci_dot_t). */
+typedef struct {
+  const double* x;
+  const double* y;
+  const double* hdiag;
+  int64_t n;
+  double e_shift;
+  int64_t out_index;
+} csffci_dot_t;
+int csffci_dots_batch(int ndots, const csffci_dot_t* dots, double* out, void* work,
+                      size_t work_bytes, cudaStream_t stream);
+
+/* y[r][:] = beta*y[r][:] + scale * sum_i coef[r*ldc+i] x[i][:], r < ny, i < nx
+ * (coef in device memory).  work: nops*sizeof(csffci_combine_t). */
+typedef struct {
+  double* y;
+  const double* x;
+  const double* coef;
+  int64_t n, ldx, ldy;
+  int32_t ny, nx, ldc, pad;
+  double beta, scale;
+  int64_t unit_begin; /* filled by the library */
+} csffci_combine_t;
+int csffci_combine_batch(int nops, csffci_combine_t* ops, void* work, size_t work_bytes,
+                         cudaStream_t stream);
+
+/* t = (r - e1 x) * P, P = capped 1/(hdiag - e_shift), e1 = ab[0]/ab[1] read
+ * on the device (ab = the two weighted dots x.P r and x.P x; NULL: e1 = 0).
+ * work: nops*sizeof(csffci_precond_t). */
+typedef struct {
+  const double* r;
+  const double* x;
+  const double* hdiag;
+  double* t;
+  const double* ab;
+  int64_t n;
+  double e_shift;
+  int64_t unit_begin; /* filled by the library */
+} csffci_precond_t;
+int csffci_precond_batch(int nops, csffci_precond_t* ops, void* work, size_t work_bytes,
+                         cudaStream_t stream);
 
 #ifdef __cplusplus
 }

@@ -35,8 +35,62 @@ class Block(ctypes.Structure):
                 ("umat", ctypes.c_void_p), ("zmat", ctypes.c_void_p)]
 
 
+class SigmaJob(ctypes.Structure):
+    """csffci_sigma_job_t."""
+    _fields_ = [("h2e", ctypes.c_void_p), ("link_a", ctypes.c_void_p), ("link_b", ctypes.c_void_p),
+                ("ci", ctypes.c_void_p), ("sigma", ctypes.c_void_p), ("scratch", ctypes.c_void_p),
+                ("neleca", ctypes.c_int32), ("nelecb", ctypes.c_int32), ("sym", ctypes.c_int32),
+                ("eta", ctypes.c_int32), ("Na", ctypes.c_int64), ("Nb", ctypes.c_int64),
+                ("unit_begin", ctypes.c_int64), ("nunits", ctypes.c_int64),
+                ("tile_begin", ctypes.c_int64), ("elem_begin", ctypes.c_int64),
+                ("nla", ctypes.c_int32), ("nlb", ctypes.c_int32)]
+
+
+class TransformJob(ctypes.Structure):
+    """csffci_transform_job_t."""
+    _fields_ = [("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("mask", ctypes.c_void_p),
+                ("umat", ctypes.c_void_p), ("ldx", ctypes.c_int64), ("ldy", ctypes.c_int64),
+                ("csd_offset", ctypes.c_int64), ("csf_offset", ctypes.c_int64), ("nconf", ctypes.c_int64),
+                ("ndet", ctypes.c_int32), ("ncsf", ctypes.c_int32), ("nvec", ctypes.c_int32),
+                ("pad", ctypes.c_int32), ("sign", ctypes.c_double), ("tile_begin", ctypes.c_int64)]
+
+
+class ZeroJob(ctypes.Structure):
+    """csffci_zero_job_t."""
+    _fields_ = [("y", ctypes.c_void_p), ("ld", ctypes.c_int64), ("n", ctypes.c_int64),
+                ("nvec", ctypes.c_int64), ("elem_begin", ctypes.c_int64)]
+
+
+class Dot(ctypes.Structure):
+    """csffci_dot_t."""
+    _fields_ = [("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("hdiag", ctypes.c_void_p),
+                ("n", ctypes.c_int64), ("e_shift", ctypes.c_double), ("out_index", ctypes.c_int64)]
+
+
+class Combine(ctypes.Structure):
+    """csffci_combine_t."""
+    _fields_ = [("y", ctypes.c_void_p), ("x", ctypes.c_void_p), ("coef", ctypes.c_void_p),
+                ("n", ctypes.c_int64), ("ldx", ctypes.c_int64), ("ldy", ctypes.c_int64),
+                ("ny", ctypes.c_int32), ("nx", ctypes.c_int32), ("ldc", ctypes.c_int32),
+                ("pad", ctypes.c_int32), ("beta", ctypes.c_double), ("scale", ctypes.c_double),
+                ("unit_begin", ctypes.c_int64)]
+
+
+class Precond(ctypes.Structure):
+    """csffci_precond_t."""
+    _fields_ = [("r", ctypes.c_void_p), ("x", ctypes.c_void_p), ("hdiag", ctypes.c_void_p),
+                ("t", ctypes.c_void_p), ("ab", ctypes.c_void_p), ("n", ctypes.c_int64),
+                ("e_shift", ctypes.c_double), ("unit_begin", ctypes.c_int64)]
+
+
 assert ctypes.sizeof(LinkEntry) == 8
 assert ctypes.sizeof(Block) == 64
+assert ctypes.sizeof(SigmaJob) == 120
+assert ctypes.sizeof(TransformJob) == 104
+assert ctypes.sizeof(ZeroJob) == 40
+assert ctypes.sizeof(Dot) == 48
+assert ctypes.sizeof(Combine) == 88
+assert ctypes.sizeof(Precond) == 64
 
 _i = ctypes.c_int
 _i64 = ctypes.c_int64
@@ -75,6 +129,12 @@ _SIGS = {
     "csffci_precond_workspace": ([], _sz),
     "csffci_precond": ([_i64, _p, _p, _p, _d, _d, _i, _d, _p, _p, _p], _i),
     "csffci_precond_dots": ([_i64, _p, _p, _p, _d, _d, _p, _p, _p], _i),
+    "csffci_sigma_batch_workspace": ([_i], _sz),
+    "csffci_sigma_batch": ([_i, _i, _p, _p, _sz, _p], _i),
+    "csffci_transform_batch": ([_i, _i, _p, _i, _p, _p, _sz, _p], _i),
+    "csffci_dots_batch": ([_i, _p, _p, _p, _sz, _p], _i),
+    "csffci_combine_batch": ([_i, _p, _p, _sz, _p], _i),
+    "csffci_precond_batch": ([_i, _p, _p, _sz, _p], _i),
 }
 
 _LIB = None

@@ -21,6 +21,7 @@
 // accesses: ds = 8 (mod 16) doubles for the m8n8k4 B fragments, LS odd for
 // the column-wise link reads.
 #include <stdlib.h>
+#include <string.h>
 
 #include "common.cuh"
 #include "profile.cuh"
@@ -46,13 +47,11 @@ __device__ __forceinline__ int rr_pair(const csffci_link_t& e) {
 }
 
 struct RRArgs {
-  const double* h2e;
-  const csffci_link_t* la;
-  const csffci_link_t* lb;
-  const double* ci;
-  double* out;
-  long long Na, Nb, nunits;
-  int npair, ds, ls, nla, nlb, nd_rows;
+  const csffci_sigma_job_t* jobs;  // device array (njobs > 1) ...
+  csffci_sigma_job_t job0;         // ... or the single job by value
+  int njobs;
+  long long total_units;
+  int npair, ds, ls, nd_rows;
   unsigned off_d, off_l, off_crow, off_las, off_rowsrc, off_zrow;
 };
 
@@ -77,7 +76,7 @@ __device__ __forceinline__ void rr_dmma8(double (&c)[4], double a0, double b) {
 
 // KS k-steps of 4 (npair rounded up to a multiple of 4); NW warps owning MW
 // (8 or 16) output rows each; NT n-tiles of 8 columns per tile.
-template <int KS, int NW, int MW, int NT, bool SYM>
+template <int KS, int NW, int MW, int NT, bool BATCH>
 __global__ void __launch_bounds__(NW * 32, 1) k_sigma_rr(RRArgs g) {
   constexpr int NTH = NW * 32;
   constexpr int NB = 8 * NT;
@@ -89,36 +88,59 @@ __global__ void __launch_bounds__(NW * 32, 1) k_sigma_rr(RRArgs g) {
   int* rowsrc = (int*)(smraw + g.off_rowsrc);  // alpha link of a pair row, -1 if none
   int* zrow = (int*)(smraw + g.off_zrow);      // [0] = count, then the rows without one
 
+  __shared__ csffci_sigma_job_t sjob_s;
+  __shared__ int sjob_idx;
+  // the single-problem launch reads its job from the parameter bank
+  const csffci_sigma_job_t& sjob = BATCH ? sjob_s : g.job0;
+
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gq = lane >> 2, tq = lane & 3;
-  const long long Nb = g.Nb;
-  const int ds = g.ds, LS = g.ls, nla = g.nla, nlb = g.nlb, npair = g.npair;
+  const int ds = g.ds, LS = g.ls, npair = g.npair;
   const int ndr = g.nd_rows;
   const size_t dsz = (size_t)ndr * ds, lsz = (size_t)NB * LS;
 
-  // h2e rows MW*w+g (and MW*w+8+g), columns 4s+t, resident for the kernel
+  // h2e rows MW*w+g (and MW*w+8+g), columns 4s+t of the current job,
+  // resident in registers until the CTA moves to another job
   double a0f[KS], a1f[MW == 16 ? KS : 1];
-  {
-    const int r0 = warp * MW + gq, r1 = r0 + 8;
-#pragma unroll
-    for (int s = 0; s < KS; ++s) {
-      const int c = 4 * s + tq;
-      a0f[s] = (r0 < npair && c < npair) ? g.h2e[(long long)r0 * npair + c] : 0.0;
-      if (MW == 16) a1f[s] = (r1 < npair && c < npair) ? g.h2e[(long long)r1 * npair + c] : 0.0;
-    }
-  }
   // rows past npair are k rows of the MMA that nothing else writes
   for (int i = tid; i < (ndr - npair) * ds; i += NTH) {
     Dbuf[npair * ds + i] = 0.0;
     Dbuf[dsz + npair * ds + i] = 0.0;
   }
+  int cur = -1;
 
-  for (long long u = blockIdx.x; u < g.nunits; u += gridDim.x) {
+  for (long long u = blockIdx.x; u < g.total_units; u += gridDim.x) {
+    if (BATCH) {
+      __syncthreads();  // everything of the previous unit is consumed
+      if (tid == 0) {
+        int j = cur < 0 ? 0 : cur;
+        while (j + 1 < g.njobs && g.jobs[j + 1].unit_begin <= u) ++j;
+        if (j != cur) sjob_s = g.jobs[j];
+        sjob_idx = j;
+      }
+      __syncthreads();
+    }
+    if ((BATCH ? sjob_idx : 0) != cur) {
+      cur = BATCH ? sjob_idx : 0;
+      const double* h2e = sjob.h2e;
+      const int r0 = warp * MW + gq, r1 = r0 + 8;
+#pragma unroll
+      for (int s = 0; s < KS; ++s) {
+        const int c = 4 * s + tq;
+        a0f[s] = (r0 < npair && c < npair) ? h2e[(long long)r0 * npair + c] : 0.0;
+        if (MW == 16) a1f[s] = (r1 < npair && c < npair) ? h2e[(long long)r1 * npair + c] : 0.0;
+      }
+    }
+    const long long Nb = sjob.Nb;
+    const int nla = sjob.nla, nlb = sjob.nlb;
+    const bool SYM = sjob.sym != 0;
+    double* const out = SYM ? sjob.scratch : sjob.sigma;
+    const long long lu = u - sjob.unit_begin;
     for (int w = 0; w < (SYM ? 2 : 1); ++w) {
-      long long ja = u;
+      long long ja = lu;
       if (SYM && w == 1) {
-        ja = g.Na - 1 - u;
-        if (ja <= u) break;
+        ja = sjob.Na - 1 - lu;
+        if (ja <= lu) break;
       }
       const long long jend = SYM ? ja + 1 : Nb;
       const int nchunk = (int)((jend + NB - 1) / NB);
@@ -126,7 +148,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_sigma_rr(RRArgs g) {
       for (int r = tid; r < ndr; r += NTH) rowsrc[r] = -1;
       __syncthreads();
       for (int l = tid; l < nla; l += NTH) {
-        csffci_link_t e = g.la[ja * nla + l];
+        csffci_link_t e = sjob.link_a[ja * nla + l];
         las[l] = e;
         rowsrc[rr_pair(e)] = l;
       }
@@ -142,7 +164,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_sigma_rr(RRArgs g) {
           if (rowsrc[r] >= 0 && las[rowsrc[r]].sign < 0) zrow[2 + n++] = r;
         zrow[1] = n;
       }
-      for (long long i = tid; i < Nb; i += NTH) cp_async8(&crow[i], &g.ci[ja * Nb + i]);
+      for (long long i = tid; i < Nb; i += NTH) cp_async8(&crow[i], &sjob.ci[ja * Nb + i]);
       {
         double* D = Dbuf;
         csffci_link_t* L = Lbuf;
@@ -151,12 +173,12 @@ __global__ void __launch_bounds__(NW * 32, 1) k_sigma_rr(RRArgs g) {
           const int l = idx / NB, jb = idx - l * NB;
           if (jb < ncol) {
             const csffci_link_t e = las[l];
-            cp_async8(&D[rr_pair(e) * ds + jb], &g.ci[(long long)e.addr * Nb + jb]);
+            cp_async8(&D[rr_pair(e) * ds + jb], &sjob.ci[(long long)e.addr * Nb + jb]);
           }
         }
         for (int idx = tid; idx < ncol * nlb; idx += NTH) {
           const int jb = idx / nlb, m = idx - jb * nlb;
-          cp_async8(&L[jb * LS + m], &g.lb[idx]);
+          cp_async8(&L[jb * LS + m], &sjob.link_b[idx]);
         }
         cp_async_commit();
       }
@@ -194,10 +216,10 @@ __global__ void __launch_bounds__(NW * 32, 1) k_sigma_rr(RRArgs g) {
             const int l = idx / NB, jb = idx - l * NB;
             if (jb < ncol2) {
               const csffci_link_t e = las[l];
-              cp_async8(&D2[rr_pair(e) * ds + jb], &g.ci[(long long)e.addr * Nb + j1 + jb]);
+              cp_async8(&D2[rr_pair(e) * ds + jb], &sjob.ci[(long long)e.addr * Nb + j1 + jb]);
             }
           }
-          const csffci_link_t* src = g.lb + j1 * nlb;
+          const csffci_link_t* src = sjob.link_b + j1 * nlb;
           for (int idx = tid; idx < ncol2 * nlb; idx += NTH) {
             const int jb = idx / nlb, m = idx - jb * nlb;
             cp_async8(&L2[jb * LS + m], &src[idx]);
@@ -240,7 +262,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_sigma_rr(RRArgs g) {
           const int m = idx / NB, jb = idx - m * NB;
           if (jb < ncol) {
             const csffci_link_t e = L[jb * LS + m];
-            atomicAdd(&g.out[ja * Nb + e.addr], e.sign * D[rr_pair(e) * ds + jb]);
+            atomicAdd(&out[ja * Nb + e.addr], e.sign * D[rr_pair(e) * ds + jb]);
           }
         }
         // alpha scatter sigma[Ka][Jb] through the links of Ja (coalesced over
@@ -250,7 +272,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_sigma_rr(RRArgs g) {
           const long long J = j0 + jb;
           if (jb < ncol && (!SYM || J < ja)) {
             const csffci_link_t e = las[l];
-            atomicAdd(&g.out[(long long)e.addr * Nb + J], e.sign * D[rr_pair(e) * ds + jb]);
+            atomicAdd(&out[(long long)e.addr * Nb + J], e.sign * D[rr_pair(e) * ds + jb]);
           }
         }
       }
@@ -258,9 +280,9 @@ __global__ void __launch_bounds__(NW * 32, 1) k_sigma_rr(RRArgs g) {
   }
 }
 
-template <int KS, int NW, int MW, int NT, bool SYM>
+template <int KS, int NW, int MW, int NT>
 static int launch_rr(RRArgs& g, size_t smem, cudaStream_t stream) {
-  auto kern = k_sigma_rr<KS, NW, MW, NT, SYM>;
+  auto kern = g.njobs > 1 ? k_sigma_rr<KS, NW, MW, NT, true> : k_sigma_rr<KS, NW, MW, NT, false>;
   CSF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, nsm = 148, per_sm = 1;
   CSF_CUDA(cudaGetDevice(&dev));
@@ -271,18 +293,19 @@ static int launch_rr(RRArgs& g, size_t smem, cudaStream_t stream) {
     return CSFFCI_ERR_INVALID;
   }
   long long grid = (long long)nsm * per_sm;
-  if (grid > g.nunits) grid = g.nunits;
+  if (grid > g.total_units) grid = g.total_units;
+  if (grid < 1) return CSFFCI_OK;
   ProfScope ps("k_sigma_rr", stream);
   kern<<<(int)grid, NW * 32, smem, stream>>>(g);
   return check_launch("sigma (register-resident)");
 }
 
-bool sigma_rr_supported(int norb) { return norb >= 8 && norb <= 16; }
+bool sigma_rr_supported(int norb) { return norb >= 4 && norb <= 16; }
 
 // (rows per warp, n-tiles): 16-row warps halve the B-fragment traffic but
 // need 2*KS + 4*NT doubles of registers per lane; with 9 warps (norb 15,16)
 // an SMSP holds 3 warps, i.e. at most 168 registers, so those sizes use
-// either 8-row warps or two n-tiles.  CSFFCI_SIGMA_MW overrides (8 or 16).
+// 8-row warps (CSFFCI_SIGMA_MW=16 selects 16-row warps with two n-tiles).
 static int rr_rows_per_warp(int norb) {
   const char* env = getenv("CSFFCI_SIGMA_MW");
   if (env && atoi(env) == 8) return 8;
@@ -290,30 +313,50 @@ static int rr_rows_per_warp(int norb) {
   return norb >= 15 ? 8 : 16;
 }
 
-int sigma_rr_run(int norb, int neleca, int nelecb, const double* h2e, const csffci_link_t* la,
-                 const csffci_link_t* lb, const double* ci, double* out, bool sym, double eta,
-                 cudaStream_t stream) {
-  (void)eta;  // the caller forms sigma = s + eta s^T
+// fill the bookkeeping fields of the jobs; returns the largest Nb, nla, nlb
+static void rr_prepare(int norb, int njobs, csffci_sigma_job_t* jobs, long long* total_units,
+                       long long* max_nb, int* max_nla, int* max_nlb) {
+  long long u = 0, t = 0, e = 0;
+  *max_nb = 0;
+  *max_nla = *max_nlb = 0;
+  for (int i = 0; i < njobs; ++i) {
+    csffci_sigma_job_t& J = jobs[i];
+    J.Na = (long long)host_binom(norb, J.neleca);
+    J.Nb = (long long)host_binom(norb, J.nelecb);
+    J.nla = J.neleca * (norb - J.neleca + 1);
+    J.nlb = J.nelecb * (norb - J.nelecb + 1);
+    J.nunits = J.sym ? (J.Na + 1) / 2 : J.Na;
+    J.unit_begin = u;
+    u += J.nunits;
+    J.tile_begin = t;
+    t += J.sym ? ((J.Na + 31) / 32) * ((J.Na + 31) / 32) : 0;
+    J.elem_begin = e;
+    e += J.Na * J.Nb;
+    if (J.Nb > *max_nb) *max_nb = J.Nb;
+    if (J.nla > *max_nla) *max_nla = J.nla;
+    if (J.nlb > *max_nlb) *max_nlb = J.nlb;
+  }
+  *total_units = u;
+}
+
+int sigma_rr_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev,
+                    const csffci_sigma_job_t& job0, long long total_units, long long max_nb,
+                    int max_nla, int max_nlb, cudaStream_t stream) {
   const int npair = norb * (norb + 1) / 2;
   const int ks = (npair + 3) / 4;
   const int mw = rr_rows_per_warp(norb);
   const int nt = (mw == 16 && norb >= 15) ? 2 : 4;
   const int nb = 8 * nt;
   RRArgs g;
-  g.h2e = h2e;
-  g.la = la;
-  g.lb = lb;
-  g.ci = ci;
-  g.out = out;
-  g.Na = (long long)host_binom(norb, neleca);
-  g.Nb = (long long)host_binom(norb, nelecb);
+  g.jobs = jobs_dev;
+  g.job0 = job0;
+  g.njobs = njobs;
+  g.total_units = total_units;
   g.npair = npair;
-  g.nla = neleca * (norb - neleca + 1);
-  g.nlb = nelecb * (norb - nelecb + 1);
-  g.ds = nb + 8;     // = 8 (mod 16)
-  g.ls = g.nlb | 1;  // odd stride
-  g.nd_rows = 4 * ks > ((npair + mw - 1) / mw) * mw ? 4 * ks : ((npair + mw - 1) / mw) * mw;
-  g.nunits = sym ? (g.Na + 1) / 2 : g.Na;
+  g.ds = nb + 8;          // = 8 (mod 16)
+  g.ls = max_nlb | 1;     // odd stride
+  const int rows_w = ((npair + mw - 1) / mw) * mw;
+  g.nd_rows = 4 * ks > rows_w ? 4 * ks : rows_w;
   size_t off = 0;
   auto take = [&](size_t bytes) {
     size_t o = off;
@@ -322,18 +365,21 @@ int sigma_rr_run(int norb, int neleca, int nelecb, const double* h2e, const csff
   };
   g.off_d = take((size_t)2 * g.nd_rows * g.ds * sizeof(double));
   g.off_l = take((size_t)2 * nb * g.ls * sizeof(csffci_link_t));
-  g.off_crow = take((size_t)g.Nb * sizeof(double));
-  g.off_las = take((size_t)(g.nla > 0 ? g.nla : 1) * sizeof(csffci_link_t));
+  g.off_crow = take((size_t)max_nb * sizeof(double));
+  g.off_las = take((size_t)(max_nla > 0 ? max_nla : 1) * sizeof(csffci_link_t));
   g.off_rowsrc = take((size_t)g.nd_rows * sizeof(int));
   g.off_zrow = take((size_t)(npair + 2) * sizeof(int));
   const size_t smem = off;
-  if (smem > 227 * 1024) {
+  if (smem > 227 * 1024 - 256) {
     set_error("sigma: tile of %zu bytes exceeds shared memory", smem);
     return CSFFCI_ERR_INVALID;
   }
-#define RR_LAUNCH(K, W, M, T) \
-  return sym ? launch_rr<K, W, M, T, true>(g, smem, stream) : launch_rr<K, W, M, T, false>(g, smem, stream)
+#define RR_LAUNCH(K, W, M, T) return launch_rr<K, W, M, T>(g, smem, stream)
   switch (norb) {
+    case 4: RR_LAUNCH(3, 1, 16, 4);
+    case 5: RR_LAUNCH(4, 1, 16, 4);
+    case 6: RR_LAUNCH(6, 2, 16, 4);
+    case 7: RR_LAUNCH(7, 2, 16, 4);
     case 8: RR_LAUNCH(9, 3, 16, 4);
     case 9: RR_LAUNCH(12, 3, 16, 4);
     case 10: RR_LAUNCH(14, 4, 16, 4);
@@ -354,4 +400,117 @@ int sigma_rr_run(int norb, int neleca, int nelecb, const double* h2e, const csff
 #undef RR_LAUNCH
 }
 
+int sigma_rr_run(int norb, int neleca, int nelecb, const double* h2e, const csffci_link_t* la,
+                 const csffci_link_t* lb, const double* ci, double* out, bool sym, double eta,
+                 cudaStream_t stream) {
+  csffci_sigma_job_t J;
+  memset(&J, 0, sizeof(J));
+  J.h2e = h2e;
+  J.link_a = la;
+  J.link_b = lb;
+  J.ci = ci;
+  J.sigma = out;
+  J.scratch = out;
+  J.neleca = neleca;
+  J.nelecb = nelecb;
+  J.sym = sym ? 1 : 0;
+  J.eta = eta < 0 ? -1 : 1;
+  long long total, maxnb;
+  int mla, mlb;
+  rr_prepare(norb, 1, &J, &total, &maxnb, &mla, &mlb);
+  return sigma_rr_launch(norb, 1, nullptr, J, total, maxnb, mla, mlb, stream);
+}
+
+// ---- batch: zero the outputs, run the jobs, form sigma = S + eta S^T -----
+__global__ void k_batch_zero(const csffci_sigma_job_t* jobs, int njobs, long long total) {
+  int j = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    while (j + 1 < njobs && jobs[j + 1].elem_begin <= i) ++j;
+    const csffci_sigma_job_t& J = jobs[j];
+    (J.sym ? J.scratch : J.sigma)[i - J.elem_begin] = 0.0;
+  }
+}
+
+__global__ void k_batch_sym_add(const csffci_sigma_job_t* jobs, int njobs, long long total_tiles) {
+  __shared__ double tile[32][33];
+  int j = 0;
+  for (long long t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+    while (j + 1 < njobs && (jobs[j + 1].tile_begin <= t || jobs[j + 1].Na == 0)) {
+      if (jobs[j + 1].tile_begin > t) break;
+      ++j;
+    }
+    while (!jobs[j].sym) ++j;  // non-symmetric jobs own no tiles
+    const csffci_sigma_job_t& J = jobs[j];
+    const long long n = J.Na;
+    const long long ntile = (n + 31) / 32;
+    const long long lt = t - J.tile_begin;
+    const long long ti = lt / ntile, tj = lt - ti * ntile;
+    const double* s = J.scratch;
+    const double eta = (double)J.eta;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      long long row = tj * 32 + r, col = ti * 32 + threadIdx.x;
+      tile[r][threadIdx.x] = (row < n && col < n) ? s[row * n + col] : 0.0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      long long row = ti * 32 + r, col = tj * 32 + threadIdx.x;
+      if (row < n && col < n) J.sigma[row * n + col] = s[row * n + col] + eta * tile[threadIdx.x][r];
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace csffci
+
+using namespace csffci;
+
+extern "C" {
+
+size_t csffci_sigma_batch_workspace(int njobs) {
+  return (size_t)(njobs > 0 ? njobs : 1) * sizeof(csffci_sigma_job_t);
+}
+
+int csffci_sigma_batch(int norb, int njobs, csffci_sigma_job_t* jobs, void* work, size_t work_bytes,
+                       cudaStream_t stream) {
+  CSF_REQUIRE(norb >= 4 && norb <= 16, "sigma_batch: norb=%d outside [4,16]", norb);
+  CSF_REQUIRE(njobs >= 0 && (njobs == 0 || jobs != nullptr), "sigma_batch: bad job list");
+  if (njobs == 0) return CSFFCI_OK;
+  for (int i = 0; i < njobs; ++i) {
+    const csffci_sigma_job_t& J = jobs[i];
+    CSF_REQUIRE(J.neleca >= 0 && J.nelecb >= 0 && J.neleca <= norb && J.nelecb <= norb,
+                "sigma_batch: job %d has bad nelec (%d,%d)", i, J.neleca, J.nelecb);
+    CSF_REQUIRE(!J.sym || (J.neleca == J.nelecb && J.scratch != nullptr && (J.eta == 1 || J.eta == -1)),
+                "sigma_batch: job %d: spin-symmetric mode needs neleca == nelecb, eta = +-1 and scratch", i);
+    CSF_REQUIRE(J.h2e && J.link_a && J.link_b && J.ci && J.sigma, "sigma_batch: job %d has a NULL pointer", i);
+  }
+  if (work == nullptr || work_bytes < csffci_sigma_batch_workspace(njobs)) {
+    set_error("sigma_batch: workspace of %zu bytes < %zu required", work_bytes,
+              csffci_sigma_batch_workspace(njobs));
+    return CSFFCI_ERR_MEMORY;
+  }
+  long long total, maxnb;
+  int mla, mlb;
+  rr_prepare(norb, njobs, jobs, &total, &maxnb, &mla, &mlb);
+  long long nelem = jobs[njobs - 1].elem_begin + jobs[njobs - 1].Na * jobs[njobs - 1].Nb;
+  long long ntiles = 0;
+  for (int i = 0; i < njobs; ++i)
+    if (jobs[i].sym) ntiles = jobs[i].tile_begin + ((jobs[i].Na + 31) / 32) * ((jobs[i].Na + 31) / 32);
+  csffci_sigma_job_t* dj = (csffci_sigma_job_t*)work;
+  CSF_CUDA(cudaMemcpyAsync(dj, jobs, njobs * sizeof(csffci_sigma_job_t), cudaMemcpyHostToDevice, stream));
+  k_batch_zero<<<grid_for(nelem, 256, 148 * 16), 256, 0, stream>>>(dj, njobs, nelem);
+  int st = check_launch("sigma_batch zero");
+  if (st) return st;
+  st = njobs > 1 ? sigma_rr_launch(norb, njobs, dj, jobs[0], total, maxnb, mla, mlb, stream)
+                 : sigma_rr_launch(norb, 1, nullptr, jobs[0], total, maxnb, mla, mlb, stream);
+  if (st) return st;
+  if (ntiles > 0) {
+    dim3 blk(32, 8);
+    ProfScope ps("k_batch_sym_add", stream);
+    k_batch_sym_add<<<grid_for(ntiles, 1, 148 * 16), blk, 0, stream>>>(dj, njobs, ntiles);
+    return check_launch("sigma_batch symmetric add");
+  }
+  return CSFFCI_OK;
+}
+
+}  // extern "C"

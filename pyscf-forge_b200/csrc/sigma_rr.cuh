@@ -1,5 +1,5 @@
 // Register-resident sigma kernel (sigma_rr.cu), used by csffci_sigma for
-// 8 <= norb <= 16.
+// 4 <= norb <= 16.
 #pragma once
 #include "common.cuh"
 
