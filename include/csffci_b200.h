@@ -202,7 +202,10 @@ int csffci_sigma(int norb, int neleca, int nelecb, const double* h2e,
 /* One sigma of a batch (csffci_sigma_batch).  The caller fills the first
  * block; the library fills the rest.  sym = 1 asserts neleca == nelecb and
  * ci = eta ci^T (the spin-symmetric kernel) and needs scratch (ndet
- * doubles); otherwise scratch may be NULL. */
+ * doubles); otherwise scratch may be NULL.  live (device, may be NULL)
+ * gates the job at run time: it runs only when live_index < *live (used by
+ * the device-resident batched solver, whose number of new vectors per
+ * problem changes from one iteration to the next). */
 typedef struct {
   const double* h2e;
   const csffci_link_t* link_a;
@@ -211,6 +214,8 @@ typedef struct {
   double* sigma;
   double* scratch;
   int32_t neleca, nelecb, sym, eta;
+  const int32_t* live;
+  int32_t live_index, pad;
   /* filled by the library */
   int64_t Na, Nb, unit_begin, nunits, tile_begin, elem_begin;
   int32_t nla, nlb;
@@ -283,7 +288,8 @@ int csffci_precond_dots(int64_t n, const double* r, const double* x, const doubl
  *      fills their bookkeeping fields, copies them into work and launches
  *      one kernel per call. ------------------------------------------------ */
 
-/* one npair block of one problem's transform over nvec vectors */
+/* one npair block of one problem's transform over nvec vectors; live
+ * (device, may be NULL) caps the vector count at run time to *live */
 typedef struct {
   const double* x;
   double* y;
@@ -292,6 +298,7 @@ typedef struct {
   int64_t ldx, ldy, csd_offset, csf_offset, nconf;
   int32_t ndet, ncsf, nvec, pad;
   double sign;
+  const int32_t* live;
   int64_t tile_begin; /* filled by the library */
 } csffci_transform_job_t;
 
@@ -352,6 +359,78 @@ typedef struct {
 } csffci_precond_t;
 int csffci_precond_batch(int nops, csffci_precond_t* ops, void* work, size_t work_bytes,
                          cudaStream_t stream);
+
+/* ---- device-resident batched solver (no counterpart in the reference;
+ *      each problem follows the one-problem Davidson of csf.py:487-490
+ *      with the diagonal Olsen preconditioner of csf.py:433) -------------
+ *
+ * A plan holds many independent problems (any norb in 4..16, electron
+ * numbers, spin and 1..8 roots each).  Every Davidson step of every
+ * problem runs on the device, driven by per-problem state records, so one
+ * iteration is a fixed launch sequence without host synchronisation; it is
+ * captured once as a CUDA graph (use_graph) and replayed, with the host
+ * reading the number of unfinished problems every check_every iterations.
+ *
+ *   create  -> arena_bytes; bind(arena) -> tables uploaded, state reset
+ *              (and, with autotune, the sigma tile shape timed per norb);
+ *   run     -> iterations; results -> energies / flags (host);
+ *   to_det  -> Ritz vectors in the determinant basis; vectors -> pointers;
+ *   destroy. */
+typedef struct {
+  int32_t norb, neleca, nelecb, nroots;
+  int32_t eta;     /* 0: general sigma; +1/-1: CSF vectors satisfy
+                      c = eta c^T (neleca == nelecb), spin-symmetric sigma */
+  int32_t nblocks; /* CSF blocks of the transformer (csffci_det2csf)       */
+  const csffci_block_t* blocks; /* host array; umat device pointers        */
+  const uint32_t* csd_mask;     /* device, ndet entries                    */
+  int64_t ncsf;
+  const double* h2e;            /* device absorbed (npair x npair)          */
+  const csffci_link_t* link_a;  /* device link tables                       */
+  const csffci_link_t* link_b;
+  const double* hdiag;          /* device CSF-basis diagonal (ncsf)         */
+  const double* x0;             /* device initial vectors (nroots x ncsf)   */
+} csffci_batch_problem_t;
+
+typedef struct {
+  double conv_tol;          /* |dE| of every root                            */
+  double conv_tol_residual; /* |r| of every root (<= 0: sqrt(conv_tol))      */
+  double lindep;            /* relative linear-dependence cut of corrections */
+  double level_shift;       /* preconditioner shift                          */
+  int32_t max_space;        /* subspace size before restart (+ nroots)       */
+  int32_t max_cycle;        /* iteration limit                               */
+  int32_t check_every;      /* iterations between completion checks          */
+  int32_t use_graph;        /* replay one captured iteration                 */
+  int32_t autotune;         /* time the sigma tile variants at bind time     */
+  int32_t pad;
+} csffci_batch_options_t;
+
+typedef struct csffci_batch_plan csffci_batch_plan_t;
+
+int csffci_batch_plan_create(int nprob, const csffci_batch_problem_t* probs,
+                             const csffci_batch_options_t* opt, csffci_batch_plan_t** plan,
+                             size_t* arena_bytes);
+/* arena: device memory of arena_bytes, 256-byte aligned, owned by the caller
+ * for the life of the plan */
+int csffci_batch_plan_bind(csffci_batch_plan_t* plan, void* arena, size_t arena_bytes,
+                           cudaStream_t stream);
+int csffci_batch_plan_run(csffci_batch_plan_t* plan, cudaStream_t stream, int* iterations);
+/* largest nroots of the batch: the row length of the result arrays */
+int csffci_batch_plan_max_roots(const csffci_batch_plan_t* plan);
+/* the sigma tile variant used per orbital count (autotuner or default):
+ * fills up to cap entries, returns the number of orbital counts */
+int csffci_batch_plan_tile_variants(const csffci_batch_plan_t* plan, int32_t* norb,
+                                    int32_t* variant, int cap);
+/* host arrays: energies/converged [nprob][max_roots] (NaN / 0 past the
+ * roots found), niter/nfound [nprob]; any may be NULL */
+int csffci_batch_plan_results(csffci_batch_plan_t* plan, double* energies, int32_t* converged,
+                              int32_t* niter, int32_t* nfound, cudaStream_t stream);
+/* Ritz vectors of every problem to the determinant basis (in the arena) */
+int csffci_batch_plan_to_det(csffci_batch_plan_t* plan, cudaStream_t stream);
+/* device addresses of problem iprob's CSF Ritz vectors (nroots x ncsf) and
+ * determinant vectors (nroots x ndet, valid after to_det) */
+int csffci_batch_plan_vectors(const csffci_batch_plan_t* plan, int iprob, const double** csf,
+                              const double** det);
+void csffci_batch_plan_destroy(csffci_batch_plan_t* plan);
 
 #ifdef __cplusplus
 }

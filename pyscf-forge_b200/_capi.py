@@ -40,7 +40,8 @@ class SigmaJob(ctypes.Structure):
     _fields_ = [("h2e", ctypes.c_void_p), ("link_a", ctypes.c_void_p), ("link_b", ctypes.c_void_p),
                 ("ci", ctypes.c_void_p), ("sigma", ctypes.c_void_p), ("scratch", ctypes.c_void_p),
                 ("neleca", ctypes.c_int32), ("nelecb", ctypes.c_int32), ("sym", ctypes.c_int32),
-                ("eta", ctypes.c_int32), ("Na", ctypes.c_int64), ("Nb", ctypes.c_int64),
+                ("eta", ctypes.c_int32), ("live", ctypes.c_void_p), ("live_index", ctypes.c_int32),
+                ("pad", ctypes.c_int32), ("Na", ctypes.c_int64), ("Nb", ctypes.c_int64),
                 ("unit_begin", ctypes.c_int64), ("nunits", ctypes.c_int64),
                 ("tile_begin", ctypes.c_int64), ("elem_begin", ctypes.c_int64),
                 ("nla", ctypes.c_int32), ("nlb", ctypes.c_int32)]
@@ -52,7 +53,8 @@ class TransformJob(ctypes.Structure):
                 ("umat", ctypes.c_void_p), ("ldx", ctypes.c_int64), ("ldy", ctypes.c_int64),
                 ("csd_offset", ctypes.c_int64), ("csf_offset", ctypes.c_int64), ("nconf", ctypes.c_int64),
                 ("ndet", ctypes.c_int32), ("ncsf", ctypes.c_int32), ("nvec", ctypes.c_int32),
-                ("pad", ctypes.c_int32), ("sign", ctypes.c_double), ("tile_begin", ctypes.c_int64)]
+                ("pad", ctypes.c_int32), ("sign", ctypes.c_double), ("live", ctypes.c_void_p),
+                ("tile_begin", ctypes.c_int64)]
 
 
 class ZeroJob(ctypes.Structure):
@@ -83,10 +85,30 @@ class Precond(ctypes.Structure):
                 ("e_shift", ctypes.c_double), ("unit_begin", ctypes.c_int64)]
 
 
+class BatchProblem(ctypes.Structure):
+    """csffci_batch_problem_t."""
+    _fields_ = [("norb", ctypes.c_int32), ("neleca", ctypes.c_int32), ("nelecb", ctypes.c_int32),
+                ("nroots", ctypes.c_int32), ("eta", ctypes.c_int32), ("nblocks", ctypes.c_int32),
+                ("blocks", ctypes.c_void_p), ("csd_mask", ctypes.c_void_p), ("ncsf", ctypes.c_int64),
+                ("h2e", ctypes.c_void_p), ("link_a", ctypes.c_void_p), ("link_b", ctypes.c_void_p),
+                ("hdiag", ctypes.c_void_p), ("x0", ctypes.c_void_p)]
+
+
+class BatchOptions(ctypes.Structure):
+    """csffci_batch_options_t."""
+    _fields_ = [("conv_tol", ctypes.c_double), ("conv_tol_residual", ctypes.c_double),
+                ("lindep", ctypes.c_double), ("level_shift", ctypes.c_double),
+                ("max_space", ctypes.c_int32), ("max_cycle", ctypes.c_int32),
+                ("check_every", ctypes.c_int32), ("use_graph", ctypes.c_int32),
+                ("autotune", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
 assert ctypes.sizeof(LinkEntry) == 8
 assert ctypes.sizeof(Block) == 64
-assert ctypes.sizeof(SigmaJob) == 120
-assert ctypes.sizeof(TransformJob) == 104
+assert ctypes.sizeof(SigmaJob) == 136
+assert ctypes.sizeof(TransformJob) == 112
+assert ctypes.sizeof(BatchProblem) == 88
+assert ctypes.sizeof(BatchOptions) == 56
 assert ctypes.sizeof(ZeroJob) == 40
 assert ctypes.sizeof(Dot) == 48
 assert ctypes.sizeof(Combine) == 88
@@ -135,6 +157,15 @@ _SIGS = {
     "csffci_dots_batch": ([_i, _p, _p, _p, _sz, _p], _i),
     "csffci_combine_batch": ([_i, _p, _p, _sz, _p], _i),
     "csffci_precond_batch": ([_i, _p, _p, _sz, _p], _i),
+    "csffci_batch_plan_create": ([_i, _p, _p, ctypes.POINTER(_p), ctypes.POINTER(_sz)], _i),
+    "csffci_batch_plan_bind": ([_p, _p, _sz, _p], _i),
+    "csffci_batch_plan_run": ([_p, _p, ctypes.POINTER(_i)], _i),
+    "csffci_batch_plan_max_roots": ([_p], _i),
+    "csffci_batch_plan_tile_variants": ([_p, _p, _p, _i], _i),
+    "csffci_batch_plan_results": ([_p, _p, _p, _p, _p, _p], _i),
+    "csffci_batch_plan_to_det": ([_p, _p], _i),
+    "csffci_batch_plan_vectors": ([_p, _i, ctypes.POINTER(_p), ctypes.POINTER(_p)], _i),
+    "csffci_batch_plan_destroy": ([_p], None),
 }
 
 _LIB = None

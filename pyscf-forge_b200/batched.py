@@ -221,7 +221,8 @@ class BatchedCSFSolver:
     """Lockstep batched CSF-basis Davidson (see the module docstring)."""
 
     def __init__(self, conv_tol=1e-10, lindep=1e-14, max_cycle=100, max_space=12, level_shift=1e-3,
-                 pspace_size=200, conv_tol_residual=None):
+                 pspace_size=200, conv_tol_residual=None, engine="device", check_every=4, use_graph=True,
+                 autotune=True):
         self.conv_tol = conv_tol
         self.lindep = lindep
         self.max_cycle = max_cycle
@@ -229,7 +230,16 @@ class BatchedCSFSolver:
         self.level_shift = level_shift
         self.pspace_size = pspace_size
         self.conv_tol_residual = conv_tol_residual
+        # "device": every Davidson step on the device (csffci_batch_plan_*,
+        # one captured iteration replayed as a CUDA graph); "host": the
+        # subspace algebra on the host between batched launches
+        self.engine = engine
+        self.check_every = check_every
+        self.use_graph = use_graph
+        self.autotune = autotune
         self.iterations = 0
+        self.niter = None
+        self.tile_variants = None
 
     # ---- batched primitives ------------------------------------------------
     def _dots(self, dots, nout):
@@ -314,9 +324,79 @@ class BatchedCSFSolver:
             S.X = torch.as_tensor(full, device=dev)
             S.e = w[:S.k]
             S.conv = [True] * S.k
-        self._davidson(states)
+        if self.engine == "device":
+            self._device_davidson(states)
+        elif self.engine == "host":
+            self._davidson(states)
+        else:
+            raise ValueError("engine must be 'device' or 'host'")
         allS = sorted(exact + states, key=lambda s: s.ip)
         return self._finish(allS, with_rdm)
+
+    def _device_davidson(self, states):
+        """All problems through one csffci_batch plan: tables built once,
+        iterations replayed on the device until every problem finished."""
+        if not states:
+            return
+        dev = device()
+        n = len(states)
+        probs = (_capi.BatchProblem * n)()
+        keep = []
+        for i, S in enumerate(states):
+            q = probs[i]
+            q.norb, q.neleca, q.nelecb, q.nroots = S.norb, S.nelec[0], S.nelec[1], S.k
+            q.eta = int(S.eta) if S.eta is not None else 0
+            blocks = S.t._c_blocks()
+            keep.append(blocks)
+            q.nblocks = len(blocks)
+            q.blocks = ctypes.addressof(blocks)
+            q.csd_mask = S.t.csd_mask.data_ptr()
+            q.ncsf = S.n
+            q.h2e, q.link_a, q.link_b = S.h2e.data_ptr(), S.la.data_ptr(), S.lb.data_ptr()
+            q.hdiag = S.hc.data_ptr()
+            x0 = torch.zeros((S.k, S.n), dtype=torch.float64, device=dev)
+            x0[torch.arange(S.k, device=dev), torch.argsort(S.hc, stable=True)[:S.k]] = 1.0
+            keep.append(x0)
+            q.x0 = x0.data_ptr()
+        opt = _capi.BatchOptions(float(self.conv_tol), float(self.conv_tol_residual or 0.0), float(self.lindep),
+                                 float(self.level_shift), int(self.max_space), int(self.max_cycle),
+                                 int(self.check_every), 1 if self.use_graph else 0, 1 if self.autotune else 0, 0)
+        plan = ctypes.c_void_p()
+        nbytes = ctypes.c_size_t()
+        _capi.call("csffci_batch_plan_create", n, probs, ctypes.byref(opt), ctypes.byref(plan), ctypes.byref(nbytes))
+        try:
+            arena = torch.empty(nbytes.value // 8 + 64, dtype=torch.float64, device=dev)
+            base = (-arena.data_ptr()) % 256 // 8
+            arena_ptr = arena.data_ptr() + 8 * base
+            _capi.call("csffci_batch_plan_bind", plan, arena_ptr, nbytes.value, stream())
+            it = ctypes.c_int()
+            _capi.call("csffci_batch_plan_run", plan, stream(), ctypes.byref(it))
+            self.iterations = it.value
+            kb = _capi.query("csffci_batch_plan_max_roots", plan)
+            e = np.empty(n * kb)
+            conv = np.zeros(n * kb, dtype=np.int32)
+            niter = np.zeros(n, dtype=np.int32)
+            nfound = np.zeros(n, dtype=np.int32)
+            _capi.call("csffci_batch_plan_results", plan, e.ctypes.data, conv.ctypes.data, niter.ctypes.data,
+                       nfound.ctypes.data, stream())
+            vn = np.zeros(32, dtype=np.int32)
+            vv = np.zeros(32, dtype=np.int32)
+            ng = _capi.query("csffci_batch_plan_tile_variants", plan, vn.ctypes.data, vv.ctypes.data, 32)
+            self.tile_variants = {int(vn[g]): int(vv[g]) for g in range(min(ng, 32))}
+            _capi.call("csffci_batch_plan_to_det", plan, stream())
+            self.niter = niter
+            for i, S in enumerate(states):
+                kk = int(nfound[i])
+                S.e = e[i * kb:i * kb + kk].copy()
+                S.conv = [bool(c) for c in conv[i * kb:i * kb + kk]]
+                csf, det = ctypes.c_void_p(), ctypes.c_void_p()
+                _capi.call("csffci_batch_plan_vectors", plan, i, ctypes.byref(csf), ctypes.byref(det))
+                oc = (csf.value - arena.data_ptr()) // 8
+                od = (det.value - arena.data_ptr()) // 8
+                S.X = arena[oc:oc + kk * S.n].view(kk, S.n).clone()
+                S.cdet_ready = arena[od:od + kk * S.ndet].view(kk, S.ndet).clone()
+        finally:
+            _capi.query("csffci_batch_plan_destroy", plan)
 
     def _davidson(self, states):
         if not states:
@@ -595,11 +675,14 @@ class BatchedCSFSolver:
     def _finish(self, allS, with_rdm):
         dev = device()
         # all eigenvectors to the determinant basis in one batched launch
-        nd = sum(S.X.shape[0] * S.ndet for S in allS)
+        nd = sum(S.X.shape[0] * S.ndet for S in allS if getattr(S, "cdet_ready", None) is None)
         dbuf = torch.empty(max(nd, 1), dtype=torch.float64, device=dev)
         o = 0
         jobs, zj = [], []
         for S in allS:
+            if getattr(S, "cdet_ready", None) is not None:
+                S.cdet = S.cdet_ready
+                continue
             S.Xc = S.X.contiguous()
             S.cdet = dbuf[o:o + S.Xc.shape[0] * S.ndet].view(S.Xc.shape[0], S.ndet)
             o += S.Xc.shape[0] * S.ndet

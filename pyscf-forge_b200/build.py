@@ -43,14 +43,26 @@ def build(force=False, verbose=False):
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
     nvcc = _nvcc()
-    objs = []
+    # headers are shared: an object is rebuilt when its source or any header
+    # is newer than it; translation units compile in parallel
+    hdr_t = max([os.path.getmtime(h) for h in glob.glob(os.path.join(SRC, "*.cuh")) +
+                 glob.glob(os.path.join(INC, "*.h"))] + [0.0])
+    objs, cmds = [], []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
-        cmd = [nvcc] + NVCC_FLAGS + ["-c", src, "-o", obj]
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.check_call(cmd)
         objs.append(obj)
+        if force or not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(src), hdr_t):
+            cmds.append([nvcc] + NVCC_FLAGS + ["-c", src, "-o", obj])
+    from concurrent.futures import ThreadPoolExecutor
+    workers = max(1, min(len(cmds), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        futs = []
+        for cmd in cmds:
+            if verbose:
+                print(" ".join(cmd))
+            futs.append(ex.submit(subprocess.check_call, cmd))
+        for f in futs:
+            f.result()
     cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB + ".tmp"] + objs
     subprocess.check_call(cmd)
     os.replace(LIB + ".tmp", LIB)

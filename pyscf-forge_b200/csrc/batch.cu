@@ -10,6 +10,7 @@
 // Every reduction runs in a fixed order (one block per dot product).
 #include "common.cuh"
 #include "profile.cuh"
+#include "batch_internal.cuh"
 
 namespace csffci {
 
@@ -34,13 +35,15 @@ __global__ void __launch_bounds__(256) k_transform_batch(const csffci_transform_
   for (int64_t tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
     while (j + 1 < njobs && jobs[j + 1].tile_begin <= tile) ++j;
     const csffci_transform_job_t& J = jobs[j];
-    const int64_t M = (int64_t)J.nvec * J.nconf;
+    const int nv = J.live ? min(J.nvec, *J.live) : J.nvec;
+    const int64_t M = (int64_t)nv * J.nconf;
     const int N = reverse ? J.ndet : J.ncsf;
     const int K = reverse ? J.ncsf : J.ndet;
     const int ntn = (N + BT_N - 1) / BT_N;
     const int64_t lt = tile - J.tile_begin;
     const int64_t m0 = (lt / ntn) * BT_M;
     const int n0 = (int)(lt % ntn) * BT_N;
+    if (m0 >= M) continue;  // rows of vectors that are not live (uniform per block)
     double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
     for (int k0 = 0; k0 < K; k0 += BT_K) {
       for (int e = tid; e < BT_M * BT_K; e += 256) {
@@ -185,6 +188,28 @@ __global__ void k_precond_batch(const csffci_precond_t* ops, int nops, int64_t t
   }
 }
 
+int transform_batch_prepare(int reverse, int njobs, csffci_transform_job_t* jobs, int64_t* total_tiles) {
+  int64_t tiles = 0;
+  for (int i = 0; i < njobs; ++i) {
+    csffci_transform_job_t& J = jobs[i];
+    CSF_REQUIRE(J.x && J.y && J.mask && J.umat && J.ncsf > 0 && J.ndet > 0, "transform_batch: job %d incomplete", i);
+    J.tile_begin = tiles;
+    const int64_t M = (int64_t)J.nvec * J.nconf;
+    const int N = reverse ? J.ndet : J.ncsf;
+    tiles += ((M + BT_M - 1) / BT_M) * ((N + BT_N - 1) / BT_N);
+  }
+  *total_tiles = tiles;
+  return CSFFCI_OK;
+}
+
+int transform_batch_launch(int reverse, const csffci_transform_job_t* jobs_dev, int njobs, int64_t tiles,
+                           cudaStream_t stream) {
+  if (tiles == 0 || njobs == 0) return CSFFCI_OK;
+  ProfScope ps("k_transform_batch", stream);
+  k_transform_batch<<<grid_for(tiles, 1, 148 * 8), 256, 0, stream>>>(jobs_dev, njobs, tiles, reverse);
+  return check_launch("transform_batch");
+}
+
 }  // namespace csffci
 
 using namespace csffci;
@@ -202,14 +227,8 @@ int csffci_transform_batch(int reverse, int njobs, csffci_transform_job_t* jobs,
     return CSFFCI_ERR_MEMORY;
   }
   int64_t tiles = 0;
-  for (int i = 0; i < njobs; ++i) {
-    csffci_transform_job_t& J = jobs[i];
-    CSF_REQUIRE(J.x && J.y && J.mask && J.umat && J.ncsf > 0 && J.ndet > 0, "transform_batch: job %d incomplete", i);
-    J.tile_begin = tiles;
-    const int64_t M = (int64_t)J.nvec * J.nconf;
-    const int N = reverse ? J.ndet : J.ncsf;
-    tiles += ((M + BT_M - 1) / BT_M) * ((N + BT_N - 1) / BT_N);
-  }
+  int st = transform_batch_prepare(reverse, njobs, jobs, &tiles);
+  if (st) return st;
   int64_t zelem = 0;
   for (int i = 0; i < nzero; ++i) {
     zjobs[i].elem_begin = zelem;
@@ -222,13 +241,10 @@ int csffci_transform_batch(int reverse, int njobs, csffci_transform_job_t* jobs,
   if (nzero) {
     CSF_CUDA(cudaMemcpyAsync(dz, zjobs, nzero * sizeof(*zjobs), cudaMemcpyHostToDevice, stream));
     k_zero_batch<<<grid_for(zelem, 256, 148 * 16), 256, 0, stream>>>(dz, nzero, zelem);
-    int st = check_launch("transform_batch zero");
+    st = check_launch("transform_batch zero");
     if (st) return st;
   }
-  if (tiles == 0) return CSFFCI_OK;
-  ProfScope ps("k_transform_batch", stream);
-  k_transform_batch<<<grid_for(tiles, 1, 148 * 8), 256, 0, stream>>>(dj, njobs, tiles, reverse);
-  return check_launch("transform_batch");
+  return transform_batch_launch(reverse, dj, njobs, tiles, stream);
 }
 
 int csffci_dots_batch(int ndots, const csffci_dot_t* dots, double* out, void* work, size_t work_bytes,

@@ -24,6 +24,9 @@ void prof_record(const char* name, cudaEvent_t a, cudaEvent_t b) { g_prof.ev[nam
 
 ProfScope::ProfScope(const char* name, cudaStream_t s) : name_(name), stream_(s), a_(nullptr), b_(nullptr) {
   if (!g_prof.on) return;
+  // launches recorded into a CUDA graph are not timed
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
   if (cudaEventCreate(&a_) != cudaSuccess || cudaEventCreate(&b_) != cudaSuccess) {
     a_ = b_ = nullptr;
     return;

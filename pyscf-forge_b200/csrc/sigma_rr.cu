@@ -23,294 +23,34 @@
 #include <stdlib.h>
 #include <string.h>
 
-#include "common.cuh"
-#include "profile.cuh"
+#include <map>
+#include <mutex>
+#include <vector>
+
 #include "sigma_rr.cuh"
+#include "sigma_rr_kernel.cuh"
 
 namespace csffci {
 
-__device__ __forceinline__ void cp_async8(void* s, const void* gsrc) {
-  unsigned sa = (unsigned)__cvta_generic_to_shared(s);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
-}
-
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-}
-
-__device__ __forceinline__ int rr_pair(const csffci_link_t& e) {
-  int p = e.op & 0xff, q = e.op >> 8;
-  int hi = p > q ? p : q, lo = p > q ? q : p;
-  return hi * (hi + 1) / 2 + lo;
-}
-
-struct RRArgs {
-  const csffci_sigma_job_t* jobs;  // device array (njobs > 1) ...
-  csffci_sigma_job_t job0;         // ... or the single job by value
-  int njobs;
-  long long total_units;
-  int npair, ds, ls, nd_rows;
-  unsigned off_d, off_l, off_crow, off_las, off_rowsrc, off_zrow;
-};
-
-
-// m16n8k4 FP64 MMA: A 16x4 (a0: row g, a1: row g+8; col t), B 4x8 (row t,
-// col g), C 16x8 (c0,c1: row g, cols 2t,2t+1; c2,c3: row g+8), g = lane/4,
-// t = lane%4.
-__device__ __forceinline__ void rr_dmma16(double (&c)[4], double a0, double a1, double b) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
-      "{%0,%1,%2,%3};\n"
-      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
-      : "d"(a0), "d"(a1), "d"(b));
-}
-
-__device__ __forceinline__ void rr_dmma8(double (&c)[4], double a0, double b) {
-  asm volatile(
-      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-      : "+d"(c[0]), "+d"(c[1])
-      : "d"(a0), "d"(b));
-}
-
-// KS k-steps of 4 (npair rounded up to a multiple of 4); NW warps owning MW
-// (8 or 16) output rows each; NT n-tiles of 8 columns per tile.
-template <int KS, int NW, int MW, int NT, bool BATCH>
-__global__ void __launch_bounds__(NW * 32, 1) k_sigma_rr(RRArgs g) {
-  constexpr int NTH = NW * 32;
-  constexpr int NB = 8 * NT;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  double* Dbuf = (double*)(smraw + g.off_d);
-  csffci_link_t* Lbuf = (csffci_link_t*)(smraw + g.off_l);
-  double* crow = (double*)(smraw + g.off_crow);
-  csffci_link_t* las = (csffci_link_t*)(smraw + g.off_las);
-  int* rowsrc = (int*)(smraw + g.off_rowsrc);  // alpha link of a pair row, -1 if none
-  int* zrow = (int*)(smraw + g.off_zrow);      // [0] = count, then the rows without one
-
-  __shared__ csffci_sigma_job_t sjob_s;
-  __shared__ int sjob_idx;
-  // the single-problem launch reads its job from the parameter bank
-  const csffci_sigma_job_t& sjob = BATCH ? sjob_s : g.job0;
-
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int gq = lane >> 2, tq = lane & 3;
-  const int ds = g.ds, LS = g.ls, npair = g.npair;
-  const int ndr = g.nd_rows;
-  const size_t dsz = (size_t)ndr * ds, lsz = (size_t)NB * LS;
-
-  // h2e rows MW*w+g (and MW*w+8+g), columns 4s+t of the current job,
-  // resident in registers until the CTA moves to another job
-  double a0f[KS], a1f[MW == 16 ? KS : 1];
-  // rows past npair are k rows of the MMA that nothing else writes
-  for (int i = tid; i < (ndr - npair) * ds; i += NTH) {
-    Dbuf[npair * ds + i] = 0.0;
-    Dbuf[dsz + npair * ds + i] = 0.0;
-  }
-  int cur = -1;
-
-  for (long long u = blockIdx.x; u < g.total_units; u += gridDim.x) {
-    if (BATCH) {
-      __syncthreads();  // everything of the previous unit is consumed
-      if (tid == 0) {
-        int j = cur < 0 ? 0 : cur;
-        while (j + 1 < g.njobs && g.jobs[j + 1].unit_begin <= u) ++j;
-        if (j != cur) sjob_s = g.jobs[j];
-        sjob_idx = j;
-      }
-      __syncthreads();
-    }
-    if ((BATCH ? sjob_idx : 0) != cur) {
-      cur = BATCH ? sjob_idx : 0;
-      const double* h2e = sjob.h2e;
-      const int r0 = warp * MW + gq, r1 = r0 + 8;
-#pragma unroll
-      for (int s = 0; s < KS; ++s) {
-        const int c = 4 * s + tq;
-        a0f[s] = (r0 < npair && c < npair) ? h2e[(long long)r0 * npair + c] : 0.0;
-        if (MW == 16) a1f[s] = (r1 < npair && c < npair) ? h2e[(long long)r1 * npair + c] : 0.0;
-      }
-    }
-    const long long Nb = sjob.Nb;
-    const int nla = sjob.nla, nlb = sjob.nlb;
-    const bool SYM = sjob.sym != 0;
-    double* const out = SYM ? sjob.scratch : sjob.sigma;
-    const long long lu = u - sjob.unit_begin;
-    for (int w = 0; w < (SYM ? 2 : 1); ++w) {
-      long long ja = lu;
-      if (SYM && w == 1) {
-        ja = sjob.Na - 1 - lu;
-        if (ja <= lu) break;
-      }
-      const long long jend = SYM ? ja + 1 : Nb;
-      const int nchunk = (int)((jend + NB - 1) / NB);
-      __syncthreads();  // the previous row is fully consumed
-      for (int r = tid; r < ndr; r += NTH) rowsrc[r] = -1;
-      __syncthreads();
-      for (int l = tid; l < nla; l += NTH) {
-        csffci_link_t e = sjob.link_a[ja * nla + l];
-        las[l] = e;
-        rowsrc[rr_pair(e)] = l;
-      }
-      __syncthreads();
-      if (tid == 0) {
-        // rows to reset each tile: first those without an alpha link (zeroed),
-        // then the alpha rows with a negative sign (negated)
-        int n = 0;
-        for (int r = 0; r < npair; ++r)
-          if (rowsrc[r] < 0) zrow[2 + n++] = r;
-        zrow[0] = n;
-        for (int r = 0; r < npair; ++r)
-          if (rowsrc[r] >= 0 && las[rowsrc[r]].sign < 0) zrow[2 + n++] = r;
-        zrow[1] = n;
-      }
-      for (long long i = tid; i < Nb; i += NTH) cp_async8(&crow[i], &sjob.ci[ja * Nb + i]);
-      {
-        double* D = Dbuf;
-        csffci_link_t* L = Lbuf;
-        const int ncol = (int)min((long long)NB, jend);
-        for (int idx = tid; idx < nla * NB; idx += NTH) {
-          const int l = idx / NB, jb = idx - l * NB;
-          if (jb < ncol) {
-            const csffci_link_t e = las[l];
-            cp_async8(&D[rr_pair(e) * ds + jb], &sjob.ci[(long long)e.addr * Nb + jb]);
-          }
-        }
-        for (int idx = tid; idx < ncol * nlb; idx += NTH) {
-          const int jb = idx / nlb, m = idx - jb * nlb;
-          cp_async8(&L[jb * LS + m], &sjob.link_b[idx]);
-        }
-        cp_async_commit();
-      }
-      for (int ch = 0; ch < nchunk; ++ch) {
-        const int b = ch & 1;
-        const long long j0 = (long long)ch * NB;
-        const int ncol = (int)min((long long)NB, jend - j0);
-        double* D = Dbuf + b * dsz;
-        csffci_link_t* L = Lbuf + b * lsz;
-        cp_async_wait_all();
-        __syncthreads();
-        // rows without an alpha link start from zero; alpha rows with a
-        // negative sign are negated (the copies brought the raw values)
-        const int nz = zrow[0], nfix = zrow[1];
-        for (int idx = tid; idx < nfix * NB; idx += NTH) {
-          const int i = idx / NB, jb = idx - i * NB;
-          double* p = &D[zrow[2 + i] * ds + jb];
-          *p = i < nz ? 0.0 : -*p;
-        }
-        __syncthreads();
-        for (int idx = tid; idx < nlb * NB; idx += NTH) {
-          const int m = idx / NB, jb = idx - m * NB;
-          if (jb < ncol) {
-            const csffci_link_t e = L[jb * LS + m];
-            D[rr_pair(e) * ds + jb] += e.sign * crow[e.addr];
-          }
-        }
-        __syncthreads();
-        if (ch + 1 < nchunk) {
-          double* D2 = Dbuf + (b ^ 1) * dsz;
-          csffci_link_t* L2 = Lbuf + (b ^ 1) * lsz;
-          const long long j1 = j0 + NB;
-          const int ncol2 = (int)min((long long)NB, jend - j1);
-          for (int idx = tid; idx < nla * NB; idx += NTH) {
-            const int l = idx / NB, jb = idx - l * NB;
-            if (jb < ncol2) {
-              const csffci_link_t e = las[l];
-              cp_async8(&D2[rr_pair(e) * ds + jb], &sjob.ci[(long long)e.addr * Nb + j1 + jb]);
-            }
-          }
-          const csffci_link_t* src = sjob.link_b + j1 * nlb;
-          for (int idx = tid; idx < ncol2 * nlb; idx += NTH) {
-            const int jb = idx / nlb, m = idx - jb * nlb;
-            cp_async8(&L2[jb * LS + m], &src[idx]);
-          }
-          cp_async_commit();
-        }
-        // V = H D on the FP64 tensor cores
-        double acc[NT][4];
-#pragma unroll
-        for (int t = 0; t < NT; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.0;
-        const double* Db = D + tq * ds + gq;
-#pragma unroll
-        for (int s = 0; s < KS; ++s) {
-          if (MW == 16) {
-#pragma unroll
-            for (int t = 0; t < NT; ++t) rr_dmma16(acc[t], a0f[s], a1f[s], Db[4 * s * ds + 8 * t]);
-          } else {
-#pragma unroll
-            for (int t = 0; t < NT; ++t) rr_dmma8(acc[t], a0f[s], Db[4 * s * ds + 8 * t]);
-          }
-        }
-        __syncthreads();
-        {
-          const int r0 = warp * MW + gq, r1 = r0 + 8;
-#pragma unroll
-          for (int t = 0; t < NT; ++t) {
-            if (r0 < npair) {
-              D[r0 * ds + 8 * t + 2 * tq] = acc[t][0];
-              D[r0 * ds + 8 * t + 2 * tq + 1] = acc[t][1];
-            }
-            if (MW == 16 && r1 < npair) {
-              D[r1 * ds + 8 * t + 2 * tq] = acc[t][2];
-              D[r1 * ds + 8 * t + 2 * tq + 1] = acc[t][3];
-            }
-          }
-        }
-        __syncthreads();
-        // row-local scatter through the beta links of each column
-        for (int idx = tid; idx < nlb * NB; idx += NTH) {
-          const int m = idx / NB, jb = idx - m * NB;
-          if (jb < ncol) {
-            const csffci_link_t e = L[jb * LS + m];
-            atomicAdd(&out[ja * Nb + e.addr], e.sign * D[rr_pair(e) * ds + jb]);
-          }
-        }
-        // alpha scatter sigma[Ka][Jb] through the links of Ja (coalesced over
-        // Jb); in the spin-symmetric mode only Jb < Ja
-        for (int idx = tid; idx < nla * NB; idx += NTH) {
-          const int l = idx / NB, jb = idx - l * NB;
-          const long long J = j0 + jb;
-          if (jb < ncol && (!SYM || J < ja)) {
-            const csffci_link_t e = las[l];
-            atomicAdd(&out[(long long)e.addr * Nb + J], e.sign * D[rr_pair(e) * ds + jb]);
-          }
-        }
-      }
-    }
-  }
-}
-
-template <int KS, int NW, int MW, int NT>
-static int launch_rr(RRArgs& g, size_t smem, cudaStream_t stream) {
-  auto kern = g.njobs > 1 ? k_sigma_rr<KS, NW, MW, NT, true> : k_sigma_rr<KS, NW, MW, NT, false>;
-  CSF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int dev = 0, nsm = 148, per_sm = 1;
-  CSF_CUDA(cudaGetDevice(&dev));
-  CSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  CSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NW * 32, smem));
-  if (per_sm < 1) {
-    set_error("sigma: register-resident kernel does not fit on an SM (smem %zu)", smem);
-    return CSFFCI_ERR_INVALID;
-  }
-  long long grid = (long long)nsm * per_sm;
-  if (grid > g.total_units) grid = g.total_units;
-  if (grid < 1) return CSFFCI_OK;
-  ProfScope ps("k_sigma_rr", stream);
-  kern<<<(int)grid, NW * 32, smem, stream>>>(g);
-  return check_launch("sigma (register-resident)");
-}
-
 bool sigma_rr_supported(int norb) { return norb >= 4 && norb <= 16; }
 
-// (rows per warp, n-tiles): 16-row warps halve the B-fragment traffic but
-// need 2*KS + 4*NT doubles of registers per lane; with 9 warps (norb 15,16)
-// an SMSP holds 3 warps, i.e. at most 168 registers, so those sizes use
-// 8-row warps (CSFFCI_SIGMA_MW=16 selects 16-row warps with two n-tiles).
-static int rr_rows_per_warp(int norb) {
-  const char* env = getenv("CSFFCI_SIGMA_MW");
-  if (env && atoi(env) == 8) return 8;
-  if (env && atoi(env) == 16) return 16;
-  return norb >= 15 ? 8 : 16;
+// Tile shapes (rows per warp, n-tiles of 8 columns): 16-row warps halve
+// the B-fragment traffic but need 2*KS + 4*NT doubles of registers per lane;
+// with 9 warps (norb 15,16) an SMSP holds 3 warps, i.e. at most 168
+// registers, so those sizes have no (16, 4) instance.  The default is
+// (16, 4) up to norb 14 and (8, 4) above; CSFFCI_SIGMA_VARIANT overrides it
+// and the batched solver's autotuner picks per orbital count.
+static const int kVariantShape[RR_NVARIANT][2] = {{16, 4}, {8, 4}, {16, 2}, {8, 2}};
+
+bool rr_variant_valid(int norb, int v) { return v >= 0 && v < RR_NVARIANT && !(v == 0 && norb >= 15); }
+
+int rr_default_variant(int norb) {
+  const char* env = getenv("CSFFCI_SIGMA_VARIANT");
+  if (env) {
+    const int v = atoi(env);
+    if (rr_variant_valid(norb, v)) return v;
+  }
+  return norb >= 15 ? 1 : 0;
 }
 
 // fill the bookkeeping fields of the jobs; returns the largest Nb, nla, nlb
@@ -341,11 +81,16 @@ static void rr_prepare(int norb, int njobs, csffci_sigma_job_t* jobs, long long*
 
 int sigma_rr_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev,
                     const csffci_sigma_job_t& job0, long long total_units, long long max_nb,
-                    int max_nla, int max_nlb, cudaStream_t stream) {
+                    int max_nla, int max_nlb, cudaStream_t stream, int variant) {
   const int npair = norb * (norb + 1) / 2;
   const int ks = (npair + 3) / 4;
-  const int mw = rr_rows_per_warp(norb);
-  const int nt = (mw == 16 && norb >= 15) ? 2 : 4;
+  if (variant < 0) variant = rr_default_variant(norb);
+  if (!rr_variant_valid(norb, variant)) {
+    set_error("sigma: tile variant %d is not available for norb=%d", variant, norb);
+    return CSFFCI_ERR_INVALID;
+  }
+  const int mw = kVariantShape[variant][0];
+  const int nt = kVariantShape[variant][1];
   const int nb = 8 * nt;
   RRArgs g;
   g.jobs = jobs_dev;
@@ -374,30 +119,12 @@ int sigma_rr_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev,
     set_error("sigma: tile of %zu bytes exceeds shared memory", smem);
     return CSFFCI_ERR_INVALID;
   }
-#define RR_LAUNCH(K, W, M, T) return launch_rr<K, W, M, T>(g, smem, stream)
-  switch (norb) {
-    case 4: RR_LAUNCH(3, 1, 16, 4);
-    case 5: RR_LAUNCH(4, 1, 16, 4);
-    case 6: RR_LAUNCH(6, 2, 16, 4);
-    case 7: RR_LAUNCH(7, 2, 16, 4);
-    case 8: RR_LAUNCH(9, 3, 16, 4);
-    case 9: RR_LAUNCH(12, 3, 16, 4);
-    case 10: RR_LAUNCH(14, 4, 16, 4);
-    case 11: RR_LAUNCH(17, 5, 16, 4);
-    case 12: RR_LAUNCH(20, 5, 16, 4);
-    case 13: RR_LAUNCH(23, 6, 16, 4);
-    case 14: RR_LAUNCH(27, 7, 16, 4);
-    case 15:
-      if (mw == 16) RR_LAUNCH(30, 8, 16, 2);
-      RR_LAUNCH(30, 15, 8, 4);
-    case 16:
-      if (mw == 16) RR_LAUNCH(34, 9, 16, 2);
-      RR_LAUNCH(34, 17, 8, 4);
-    default:
-      set_error("sigma: no register-resident instance for norb=%d", norb);
-      return CSFFCI_ERR_INVALID;
+switch (variant) {
+    case 0: return rr_dispatch_v0(norb, g, smem, stream);
+    case 1: return rr_dispatch_v1(norb, g, smem, stream);
+    case 2: return rr_dispatch_v2(norb, g, smem, stream);
+    default: return rr_dispatch_v3(norb, g, smem, stream);
   }
-#undef RR_LAUNCH
 }
 
 int sigma_rr_run(int norb, int neleca, int nelecb, const double* h2e, const csffci_link_t* la,
@@ -418,16 +145,21 @@ int sigma_rr_run(int norb, int neleca, int nelecb, const double* h2e, const csff
   long long total, maxnb;
   int mla, mlb;
   rr_prepare(norb, 1, &J, &total, &maxnb, &mla, &mlb);
-  return sigma_rr_launch(norb, 1, nullptr, J, total, maxnb, mla, mlb, stream);
+  return sigma_rr_launch(norb, 1, nullptr, J, total, maxnb, mla, mlb, stream, -1);
 }
 
 // ---- batch: zero the outputs, run the jobs, form sigma = S + eta S^T -----
+__device__ __forceinline__ bool job_live(const csffci_sigma_job_t& J) {
+  return J.live == nullptr || J.live_index < *J.live;
+}
+
 __global__ void k_batch_zero(const csffci_sigma_job_t* jobs, int njobs, long long total) {
   int j = 0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
     while (j + 1 < njobs && jobs[j + 1].elem_begin <= i) ++j;
     const csffci_sigma_job_t& J = jobs[j];
+    if (!job_live(J)) continue;
     (J.sym ? J.scratch : J.sigma)[i - J.elem_begin] = 0.0;
   }
 }
@@ -442,6 +174,7 @@ __global__ void k_batch_sym_add(const csffci_sigma_job_t* jobs, int njobs, long 
     }
     while (!jobs[j].sym) ++j;  // non-symmetric jobs own no tiles
     const csffci_sigma_job_t& J = jobs[j];
+    if (!job_live(J)) continue;  // uniform over the block (one tile per block)
     const long long n = J.Na;
     const long long ntile = (n + 31) / 32;
     const long long lt = t - J.tile_begin;
@@ -461,6 +194,110 @@ __global__ void k_batch_sym_add(const csffci_sigma_job_t* jobs, int njobs, long 
   }
 }
 
+int sigma_batch_prepare(int norb, int njobs, csffci_sigma_job_t* jobs, SigmaBatchInfo* info) {
+  CSF_REQUIRE(norb >= 4 && norb <= 16, "sigma_batch: norb=%d outside [4,16]", norb);
+  CSF_REQUIRE(njobs > 0 && jobs != nullptr, "sigma_batch: bad job list");
+  for (int i = 0; i < njobs; ++i) {
+    const csffci_sigma_job_t& J = jobs[i];
+    CSF_REQUIRE(J.neleca >= 0 && J.nelecb >= 0 && J.neleca <= norb && J.nelecb <= norb,
+                "sigma_batch: job %d has bad nelec (%d,%d)", i, J.neleca, J.nelecb);
+    CSF_REQUIRE(!J.sym || (J.neleca == J.nelecb && J.scratch != nullptr && (J.eta == 1 || J.eta == -1)),
+                "sigma_batch: job %d: spin-symmetric mode needs neleca == nelecb, eta = +-1 and scratch", i);
+    CSF_REQUIRE(J.h2e && J.link_a && J.link_b && J.ci && J.sigma, "sigma_batch: job %d has a NULL pointer", i);
+  }
+  info->norb = norb;
+  info->njobs = njobs;
+  rr_prepare(norb, njobs, jobs, &info->total_units, &info->max_nb, &info->max_nla, &info->max_nlb);
+  info->nelem = jobs[njobs - 1].elem_begin + jobs[njobs - 1].Na * jobs[njobs - 1].Nb;
+  info->ntiles = 0;
+  for (int i = 0; i < njobs; ++i)
+    if (jobs[i].sym) info->ntiles = jobs[i].tile_begin + ((jobs[i].Na + 31) / 32) * ((jobs[i].Na + 31) / 32);
+  info->job0 = jobs[0];
+  return CSFFCI_OK;
+}
+
+int sigma_batch_launch(const SigmaBatchInfo& info, const csffci_sigma_job_t* dj, cudaStream_t stream) {
+  const int njobs = info.njobs;
+  if (njobs == 0) return CSFFCI_OK;
+  k_batch_zero<<<grid_for(info.nelem, 256, 148 * 16), 256, 0, stream>>>(dj, njobs, info.nelem);
+  int st = check_launch("sigma_batch zero");
+  if (st) return st;
+  // a gated single job goes through the job-table kernel (the by-value
+  // form cannot see the gate)
+  const bool table = njobs > 1 || info.job0.live != nullptr;
+  st = table ? sigma_rr_launch(info.norb, njobs, dj, info.job0, info.total_units, info.max_nb,
+                               info.max_nla, info.max_nlb, stream, info.variant)
+             : sigma_rr_launch(info.norb, 1, nullptr, info.job0, info.total_units, info.max_nb,
+                               info.max_nla, info.max_nlb, stream, info.variant);
+  if (st) return st;
+  if (info.ntiles > 0) {
+    dim3 blk(32, 8);
+    ProfScope ps("k_batch_sym_add", stream);
+    k_batch_sym_add<<<grid_for(info.ntiles, 1, 148 * 16), blk, 0, stream>>>(dj, njobs, info.ntiles);
+    return check_launch("sigma_batch symmetric add");
+  }
+  return CSFFCI_OK;
+}
+
+// ---- autotuner: the fastest tile variant per (norb, job-shape signature),
+//      timed on the caller's job table and cached for the process ---------
+static std::mutex g_tune_mu;
+static std::map<std::pair<int, unsigned long long>, int> g_tune_cache;
+
+static unsigned long long job_signature(const csffci_sigma_job_t* jobs, int njobs) {
+  unsigned long long h = 1469598103934665603ull;  // FNV-1a
+  auto mix = [&](unsigned long long v) {
+    h ^= v;
+    h *= 1099511628211ull;
+  };
+  mix((unsigned long long)njobs);
+  for (int i = 0; i < njobs; ++i)
+    mix(((unsigned long long)jobs[i].neleca << 16) | ((unsigned long long)jobs[i].nelecb << 8) |
+        (unsigned long long)jobs[i].sym);
+  return h;
+}
+
+int sigma_batch_tune(SigmaBatchInfo& info, const csffci_sigma_job_t* jobs_host, const csffci_sigma_job_t* dj,
+                     cudaStream_t stream) {
+  const auto key = std::make_pair(info.norb, job_signature(jobs_host, info.njobs));
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      info.variant = it->second;
+      return CSFFCI_OK;
+    }
+  }
+  cudaEvent_t a, b;
+  CSF_CUDA(cudaEventCreate(&a));
+  CSF_CUDA(cudaEventCreate(&b));
+  int best = rr_default_variant(info.norb);
+  float best_ms = 1e30f;
+  for (int v = 0; v < RR_NVARIANT; ++v) {
+    if (!rr_variant_valid(info.norb, v)) continue;
+    SigmaBatchInfo t = info;
+    t.variant = v;
+    if (sigma_batch_launch(t, dj, stream) != CSFFCI_OK) continue;  // e.g. shared memory too small
+    cudaEventRecord(a, stream);
+    int st = sigma_batch_launch(t, dj, stream);
+    if (st == CSFFCI_OK) st = sigma_batch_launch(t, dj, stream);
+    cudaEventRecord(b, stream);
+    if (cudaEventSynchronize(b) != cudaSuccess || st != CSFFCI_OK) continue;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  info.variant = best;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[key] = best;
+  return CSFFCI_OK;
+}
+
 }  // namespace csffci
 
 using namespace csffci;
@@ -473,44 +310,19 @@ size_t csffci_sigma_batch_workspace(int njobs) {
 
 int csffci_sigma_batch(int norb, int njobs, csffci_sigma_job_t* jobs, void* work, size_t work_bytes,
                        cudaStream_t stream) {
-  CSF_REQUIRE(norb >= 4 && norb <= 16, "sigma_batch: norb=%d outside [4,16]", norb);
   CSF_REQUIRE(njobs >= 0 && (njobs == 0 || jobs != nullptr), "sigma_batch: bad job list");
   if (njobs == 0) return CSFFCI_OK;
-  for (int i = 0; i < njobs; ++i) {
-    const csffci_sigma_job_t& J = jobs[i];
-    CSF_REQUIRE(J.neleca >= 0 && J.nelecb >= 0 && J.neleca <= norb && J.nelecb <= norb,
-                "sigma_batch: job %d has bad nelec (%d,%d)", i, J.neleca, J.nelecb);
-    CSF_REQUIRE(!J.sym || (J.neleca == J.nelecb && J.scratch != nullptr && (J.eta == 1 || J.eta == -1)),
-                "sigma_batch: job %d: spin-symmetric mode needs neleca == nelecb, eta = +-1 and scratch", i);
-    CSF_REQUIRE(J.h2e && J.link_a && J.link_b && J.ci && J.sigma, "sigma_batch: job %d has a NULL pointer", i);
-  }
   if (work == nullptr || work_bytes < csffci_sigma_batch_workspace(njobs)) {
     set_error("sigma_batch: workspace of %zu bytes < %zu required", work_bytes,
               csffci_sigma_batch_workspace(njobs));
     return CSFFCI_ERR_MEMORY;
   }
-  long long total, maxnb;
-  int mla, mlb;
-  rr_prepare(norb, njobs, jobs, &total, &maxnb, &mla, &mlb);
-  long long nelem = jobs[njobs - 1].elem_begin + jobs[njobs - 1].Na * jobs[njobs - 1].Nb;
-  long long ntiles = 0;
-  for (int i = 0; i < njobs; ++i)
-    if (jobs[i].sym) ntiles = jobs[i].tile_begin + ((jobs[i].Na + 31) / 32) * ((jobs[i].Na + 31) / 32);
+  SigmaBatchInfo info;
+  int st = sigma_batch_prepare(norb, njobs, jobs, &info);
+  if (st) return st;
   csffci_sigma_job_t* dj = (csffci_sigma_job_t*)work;
   CSF_CUDA(cudaMemcpyAsync(dj, jobs, njobs * sizeof(csffci_sigma_job_t), cudaMemcpyHostToDevice, stream));
-  k_batch_zero<<<grid_for(nelem, 256, 148 * 16), 256, 0, stream>>>(dj, njobs, nelem);
-  int st = check_launch("sigma_batch zero");
-  if (st) return st;
-  st = njobs > 1 ? sigma_rr_launch(norb, njobs, dj, jobs[0], total, maxnb, mla, mlb, stream)
-                 : sigma_rr_launch(norb, 1, nullptr, jobs[0], total, maxnb, mla, mlb, stream);
-  if (st) return st;
-  if (ntiles > 0) {
-    dim3 blk(32, 8);
-    ProfScope ps("k_batch_sym_add", stream);
-    k_batch_sym_add<<<grid_for(ntiles, 1, 148 * 16), blk, 0, stream>>>(dj, njobs, ntiles);
-    return check_launch("sigma_batch symmetric add");
-  }
-  return CSFFCI_OK;
+  return sigma_batch_launch(info, dj, stream);
 }
 
 }  // extern "C"

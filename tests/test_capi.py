@@ -33,3 +33,38 @@ def test_struct_layouts():
     from pyscf_forge_b200 import _capi
     assert ctypes.sizeof(_capi.LinkEntry) == 8
     assert ctypes.sizeof(_capi.Block) == 64
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """sizeof/offsetof of every descriptor struct of include/csffci_b200.h,
+    compiled by the host C compiler, equal the ctypes mirrors."""
+    import shutil
+    import subprocess
+    import pytest
+    from pyscf_forge_b200 import _capi
+    cc = shutil.which("gcc") or shutil.which("cc")
+    cuda_inc = "/usr/local/cuda/include"
+    if cc is None or not os.path.exists(os.path.join(cuda_inc, "cuda_runtime.h")):
+        pytest.skip("no host C compiler or CUDA headers")
+    structs = {"csffci_link_t": _capi.LinkEntry, "csffci_block_t": _capi.Block,
+               "csffci_sigma_job_t": _capi.SigmaJob, "csffci_transform_job_t": _capi.TransformJob,
+               "csffci_zero_job_t": _capi.ZeroJob, "csffci_dot_t": _capi.Dot,
+               "csffci_combine_t": _capi.Combine, "csffci_precond_t": _capi.Precond,
+               "csffci_batch_problem_t": _capi.BatchProblem, "csffci_batch_options_t": _capi.BatchOptions}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "csffci_b200.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append('printf("%s %%zu\\n", sizeof(%s));' % (cname, cname))
+        for f in py._fields_:
+            lines.append('printf("%s.%s %%zu\\n", offsetof(%s, %s));' % (cname, f[0], cname, f[0]))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), "-I", cuda_inc, str(src), "-o", str(exe)],
+                   check=True)
+    out = dict(l.split() for l in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                   text=True).stdout.splitlines())
+    for cname, py in structs.items():
+        assert int(out[cname]) == ctypes.sizeof(py), cname
+        for f in py._fields_:
+            assert int(out[cname + "." + f[0]]) == getattr(py, f[0]).offset, (cname, f[0])
