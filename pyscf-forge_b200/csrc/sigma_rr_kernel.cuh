@@ -58,8 +58,17 @@ __device__ __forceinline__ void rr_dmma8(double (&c)[4], double a0, double b) {
 
 // KS k-steps of 4 (npair rounded up to a multiple of 4); NW warps owning MW
 // (8 or 16) output rows each; NT n-tiles of 8 columns per tile.
+// CTAs per SM the register allocation is sized for: the (16, 4) and (8, 4)
+// shapes keep every register they need (one CTA per SM); the two-n-tile
+// shapes cap registers so that small orbital counts, whose CTAs have few
+// warps, run two or three CTAs per SM.
+template <int NW, int MW, int NT>
+constexpr int rr_min_blocks() {
+  return NT == 2 ? (MW == 16 ? (NW <= 5 ? 3 : NW <= 6 ? 2 : 1) : (NW <= 10 ? 2 : 1)) : 1;
+}
+
 template <int KS, int NW, int MW, int NT, bool BATCH>
-__global__ void __launch_bounds__(NW * 32, 1) k_sigma_rr(RRArgs g) {
+__global__ void __launch_bounds__(NW * 32, (rr_min_blocks<NW, MW, NT>())) k_sigma_rr(RRArgs g) {
   constexpr int NTH = NW * 32;
   constexpr int NB = 8 * NT;
   extern __shared__ __align__(16) unsigned char smraw[];
