@@ -16,6 +16,10 @@ region).  ``roofline`` reports the sigma kernel against HBM with the
 algorithmic bytes 8*ndet*2*(nlink_a+nlink_b) per launch.  N>1: independent
 replicas, one per GPU (the path does not shard); value is the sum.
 
+``batched`` (same line, rank 0 at N=1): solves+RDMs/s of 128 seeded uneven
+problems through the device-resident batched solver, next to the plain
+one-problem-at-a-time GPU form on the same problems (run_batched).
+
 Reference arm: the reference's own CPU sigma (pyscf/lib/mcscf GAS library
 with one subspace, built into oracle/_ref) on all host cores.
 """
@@ -313,8 +317,50 @@ def run_ours(args, rank_env):
         v, cores, sample = cpu_reference_sigma(NORB, NELEC, RANK, budget_s=20.0)
         line["cpu_baseline"] = {"value": v, "unit": "sigma/s", "cores": cores, "kind": "reference",
                                 "sample": sample}
+    if rank == 0 and world == 1 and not args.no_batched:
+        line["batched"] = run_batched(args.batch)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def run_batched(nprob):
+    """Batched uneven solves: nprob seeded problems (norb 6..12, 1-4 roots,
+    several spins), energies and 1-/2-RDMs of every root, through the
+    device-resident batched solver (one captured Davidson iteration replayed
+    for all problems) and through the plain one-problem-at-a-time GPU form
+    (FCISolver.kernel + make_rdm12 per problem).  Both are end to end: host
+    integrals in, host energies / CI vectors / RDMs out.  Solver settings
+    are the reference's defaults (conv_tol 1e-10, residual sqrt(conv_tol),
+    max_space 12, level shift 1e-3) with max_cycle 400."""
+    import numpy as np
+    import torch
+    from pyscf_forge_b200 import batched as Bt
+    probs = Bt.make_uneven_batch(nprob)
+    kw = dict(conv_tol=1e-10, max_cycle=400)
+    Bt.BatchedCSFSolver(**kw).kernel(probs)  # warm-up: transformers, autotuner
+    Bt.solve_plain(probs[:8], **kw)
+    torch.cuda.synchronize()
+    sol = Bt.BatchedCSFSolver(**kw)
+    t0 = time.perf_counter()
+    rb = sol.kernel(probs)
+    torch.cuda.synchronize()
+    tb = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    rp = Bt.solve_plain(probs, **kw)
+    torch.cuda.synchronize()
+    tp = time.perf_counter() - t0
+    de = max(float(np.max(np.abs(a[0] - b[0]))) for a, b in zip(rb, rp))
+    nroots = sum(len(a[0]) for a in rb)
+    return {"metric": "batched solves+RDMs/s", "value": nprob / tb, "unit": "solves/s",
+            "plain_value": nprob / tp, "speedup_vs_plain": tp / tb, "seconds": tb, "plain_seconds": tp,
+            "problems": nprob, "roots": nroots, "converged_problems": int(sum(bool(a[3]) for a in rb)),
+            "iterations": sol.iterations, "max_abs_dE_vs_plain": de,
+            "tile_variants": {str(k): v for k, v in (sol.tile_variants or {}).items()},
+            "config": {"workload": "%d uneven problems, norb 6..12, nelec within +-2 of half filling, "
+                                   "S in {0,1,2}, 1-4 roots, seeded rank-2*norb integrals" % nprob,
+                       "solver": "conv_tol 1e-10, max_cycle 400, max_space 12",
+                       "plain": "FCISolver.kernel + make_rdm12 per root, one problem at a time",
+                       "e2e": "host integrals in, host energies/CI/RDMs out (both forms)"}}
 
 
 def main():
@@ -327,6 +373,8 @@ def main():
     ap.add_argument("--workload", default="cas16", choices=sorted(WORKLOADS),
                     help="cas16 is the benchmark; the smaller ones exist for profiling captures")
     ap.add_argument("--no-e2e", action="store_true", help="time the device loop only (profiling)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-solves measurement")
+    ap.add_argument("--batch", type=int, default=128, help="problems in the batched-solves measurement")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
