@@ -41,9 +41,10 @@ METRIC = "CAS(16,16) FP64 sigma/s"
 WORKLOADS = {"cas16": (16, (8, 8), 32), "cas14": (14, (7, 7), 28), "cas12": (12, (6, 6), 24)}
 
 
-# DRAM bytes (read + write) per k_sigma_rr launch from ncu (profiles/); None
-# until captured for the current kernel
-TRAFFIC = {}
+# DRAM bytes (read + write) per k_sigma_rr launch from one ncu capture of
+# the full-size launch (profiles/k_sigma_rr_cas16_dram.md); None for the
+# profiling workloads that were not captured at full size
+TRAFFIC = {"cas16": 26918464000 + 13334911744}
 
 
 def seeded_integrals(norb, rank, seed=0):
