@@ -66,6 +66,13 @@ typedef struct {
   const double* zmat;  /* device f64[nspin*(nspin-1)/2][ncsf] exchange
                           expectation table for hdiag_csf (may be NULL for
                           transforms)                                        */
+  const int32_t* conf_sel; /* NULL: all configurations of the block.  Else
+                          device int32[nconf]: the block's configurations
+                          (indices within the block, ascending) that belong
+                          to the wavefunction's point-group irrep; nconf and
+                          csf_offset then count in the packed CSF vector of
+                          the symmetric solver (csf_symm.py:25-107,
+                          csfstring.py:74-103 pack_csf/unpack_csf).         */
 } csffci_block_t;
 
 int csffci_abi_version(void);

@@ -241,6 +241,28 @@ def make_econf_csf_mask(norb, neleca, nelecb, smult):
     return np.concatenate(parts).astype(np.uint32)
 
 
+def strs_irrep(strs, orbsym):
+    """Irrep of each occupation string for D2h-subgroup irrep ids: XOR of
+    the irreps of the occupied orbitals (the role of
+    direct_spin1_symm._gen_strs_irrep at csfstring.py:280-285)."""
+    strs = np.asarray(strs, dtype=np.int64)
+    out = np.zeros(strs.shape, dtype=np.int64)
+    for p, s in enumerate((np.asarray(orbsym, dtype=np.int64) % 10).tolist()):
+        out ^= ((strs >> p) & 1) * s
+    return out
+
+
+def make_confsym(norb, neleca, nelecb, econf_det_mask, orbsym):
+    """csfstring.py:278-290: irrep of every configuration, read from one
+    determinant of it (alpha-string irrep XOR beta-string irrep)."""
+    ia = strs_irrep(gen_strings(norb, neleca), orbsym)
+    ib = strs_irrep(gen_strings(norb, nelecb), orbsym)
+    econf_det_mask = np.asarray(econf_det_mask, dtype=np.int64)
+    nconf, addr = np.unique(econf_det_mask, return_index=True)
+    nb = ib.size
+    return ia[addr // nb] ^ ib[addr % nb]
+
+
 def gen_addrs2str(nspin, smult, addrs):
     """csfstring.c:243-293 (coupling string of a genealogical address)."""
     g = csf_gentable(nspin, smult)

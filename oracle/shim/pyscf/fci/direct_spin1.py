@@ -33,7 +33,7 @@ def _get_init_guess(na, nb, nroots, hdiag, nelec):
     for a in addrs:
         x = np.zeros(na * nb)
         x[a] = 1.0
-        ci0.append(x.reshape(na, nb))
+        ci0.append(x)  # flat vectors, as PySCF returns them
     return ci0
 
 

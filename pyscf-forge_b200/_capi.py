@@ -32,7 +32,7 @@ class Block(ctypes.Structure):
     _fields_ = [("csd_offset", ctypes.c_int64), ("csf_offset", ctypes.c_int64),
                 ("nconf", ctypes.c_int64), ("ndet", ctypes.c_int32), ("ncsf", ctypes.c_int32),
                 ("nspin", ctypes.c_int32), ("npair", ctypes.c_int32), ("sign", ctypes.c_double),
-                ("umat", ctypes.c_void_p), ("zmat", ctypes.c_void_p)]
+                ("umat", ctypes.c_void_p), ("zmat", ctypes.c_void_p), ("conf_sel", ctypes.c_void_p)]
 
 
 class SigmaJob(ctypes.Structure):
@@ -104,7 +104,7 @@ class BatchOptions(ctypes.Structure):
 
 
 assert ctypes.sizeof(LinkEntry) == 8
-assert ctypes.sizeof(Block) == 64
+assert ctypes.sizeof(Block) == 72
 assert ctypes.sizeof(SigmaJob) == 136
 assert ctypes.sizeof(TransformJob) == 112
 assert ctypes.sizeof(BatchProblem) == 88

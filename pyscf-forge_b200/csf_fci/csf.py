@@ -138,12 +138,18 @@ def pspace(fci, h1e, eri, norb, nelec, transformer, hdiag_det=None, hdiag_csf=No
     if hdiag_csf is None:
         hdiag_csf = make_hdiag_csf(h1e, eri, norb, nelec, transformer, hdiag_det=hdiag_det)
     hdiag_csf = to_dev(hdiag_csf).reshape(-1)
-    ncsf = hdiag_csf.numel()
     npsp = int(npsp)
+    # candidates: every CSF, or those of the irrep wfnsym (csf.py:266-271);
+    # addresses stay in the full CSF numbering, as the reference returns them
+    idx_sym = transformer.idx_sym
+    cand = torch.arange(hdiag_csf.numel(), device=hdiag_csf.device)
+    if idx_sym is not None:
+        cand = cand[idx_sym]
+    ncsf = cand.numel()
     if ncsf > npsp:
-        csf_addr = torch.argsort(hdiag_csf, stable=True)[:npsp]
+        csf_addr = cand[torch.argsort(hdiag_csf[cand], stable=True)[:npsp]]
     else:
-        csf_addr = torch.arange(ncsf, device=hdiag_csf.device)
+        csf_addr = cand
     npsp_csf = csf_addr.numel()
     econf = torch.unique(transformer.econf_csf_mask[csf_addr].long()).cpu().numpy()
     det_addr = _conf_dets(transformer, econf)
@@ -163,8 +169,11 @@ def pspace(fci, h1e, eri, norb, nelec, transformer, hdiag_det=None, hdiag_csf=No
 
 def get_init_guess(norb, nelec, nroots, hdiag_csf, transformer):
     """csf.py:51-64: unit vectors on the lowest diagonal CSFs (CSF basis,
-    device)."""
+    device; the packed symmetric CSF basis when the transformer has a
+    point group, from the full diagonal)."""
     hd = to_dev(hdiag_csf).reshape(-1)
+    if transformer.idx_sym is not None and hd.numel() != transformer.ncsf:
+        hd = transformer.pack_csf(hd)
     ncsf = hd.numel()
     assert ncsf >= nroots, "Can't find {} roots among only {} CSFs".format(nroots, ncsf)
     addr = torch.argsort(hd, stable=True)[:nroots]
@@ -205,8 +214,6 @@ def kernel(fci, h1e, eri, norb, nelec, smult=None, idx_sym=None, ci0=None, tol=N
            max_memory=None, orbsym=None, wfnsym=None, ecore=0, transformer=None, **kwargs):
     """csf.py:368-497."""
     require_cuda()
-    if idx_sym is not None:
-        raise NotImplementedError("point-group symmetry (csf_symm) is not implemented")
     kwargs.pop('verbose', None)
     if nroots is None:
         nroots = fci.nroots
@@ -222,7 +229,18 @@ def kernel(fci, h1e, eri, norb, nelec, smult=None, idx_sym=None, ci0=None, tol=N
     hdiag_det = make_hdiag_det(fci, h1e, eri, norb, nelec)
     hdiag_csf = make_hdiag_csf(h1e, eri, norb, nelec, transformer, hdiag_det=hdiag_det)
     ncsf_all = count_all_csfs(norb, neleca, nelecb, smult)
-    ncsf_sym = ncsf_all
+    if idx_sym is None:
+        idx_sym = transformer.idx_sym
+    if idx_sym is None:
+        ncsf_sym = ncsf_all
+        pos = None
+    else:
+        # Davidson runs in the packed space of the CSFs of irrep wfnsym
+        # (csf.py:391-394, 431-437); pos maps full CSF addresses to it
+        idx_sym = to_dev(idx_sym).to(torch.bool)
+        ncsf_sym = int(idx_sym.sum().item())
+        pos = (torch.cumsum(idx_sym.to(torch.int64), 0) - 1).cpu().numpy()
+    assert ncsf_sym > 0, "Can't find {} roots among only 0 CSFs".format(nroots)
     nroots = min(ncsf_sym, nroots)
     na, nb = comb(norb, neleca), comb(norb, nelecb)
     addr, h0 = fci.pspace(h1e, eri, norb, nelec, hdiag_det=hdiag_det, hdiag_csf=hdiag_csf,
@@ -240,7 +258,7 @@ def kernel(fci, h1e, eri, norb, nelec, smult=None, idx_sym=None, ci0=None, tol=N
             return pw[0] + ecore, civec.reshape(na, nb)
         order = np.argsort(addr)
         pv_full = np.zeros((ncsf_sym, pv.shape[1]))
-        pv_full[addr] = pv
+        pv_full[addr if pos is None else pos[addr]] = pv
         if nroots > 1:
             civec = transformer.dev_csf2det(torch.as_tensor(pv_full[:, :nroots].T.copy(), device=device()))
             return pw[:nroots] + ecore, [c.reshape(na, nb) for c in civec]
@@ -249,7 +267,10 @@ def kernel(fci, h1e, eri, norb, nelec, smult=None, idx_sym=None, ci0=None, tol=N
             return pw[0] + ecore, civec.reshape(na, nb)
         del order
 
-    precond = fci.make_precond(hdiag_csf, pw, pv, addr)
+    if pos is None:
+        precond = fci.make_precond(hdiag_csf, pw, pv, addr)
+    else:
+        precond = fci.make_precond(to_dev(hdiag_csf).reshape(-1)[idx_sym], pw, pv, pos[addr])
     h2e = fci.absorb_h1e(h1e, eri, norb, nelec, .5)
     if not isinstance(h2e, H2eff):
         h2e = H2eff(to_dev(eri_pair_matrix(h2e, norb)))

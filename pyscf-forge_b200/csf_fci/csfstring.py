@@ -167,13 +167,14 @@ class CSFTransformer:
 
     def __init__(self, norb, neleca, nelecb, smult, orbsym=None, wfnsym=None, max_memory=None):
         require_cuda()
-        if orbsym is not None and wfnsym is not None:
-            raise NotImplementedError("point-group symmetry (csf_symm) is not implemented")
         self._norb = self._neleca = self._nelecb = self._smult = None
-        self._orbsym = orbsym
+        self._orbsym = None
+        self.confsym = None
+        self._symcache = {}
         self.wfnsym = wfnsym
         self.max_memory = max_memory
         self._update_spin_cache(norb, neleca, nelecb, smult)
+        self.orbsym = orbsym
 
     # ---- cache -----------------------------------------------------------
     def _update_spin_cache(self, norb, neleca, nelecb, smult):
@@ -204,8 +205,60 @@ class CSFTransformer:
         self._cblocks = None
         self._eta = None
         self._shape_info = (min_npair, csf_off, dconf, sconf, ncsf_b)
+        self._symcache = {}
+        if self._orbsym is not None:
+            self.confsym = make_confsym(norb, neleca, nelecb, self.econf_det_mask, self._orbsym)
 
-    def _c_blocks(self, with_zmat=False):
+    def _update_symm_cache(self, orbsym):
+        """csfstring.py:117-120: configuration irreps for a new orbsym."""
+        if orbsym is not None:
+            orbsym = np.asarray(orbsym, dtype=np.int64)
+        changed = (orbsym is None) != (self._orbsym is None) or (
+            orbsym is not None and (orbsym.shape != self._orbsym.shape or np.any(orbsym != self._orbsym)))
+        if orbsym is not None and (self.confsym is None or changed):
+            self.confsym = make_confsym(self._norb, self._neleca, self._nelecb, self.econf_det_mask, orbsym)
+        if changed:
+            self._symcache = {}
+        if orbsym is None:
+            self.confsym = None
+        self._orbsym = orbsym
+
+    def _sym(self):
+        """Packing of the CSF vector to the CSFs whose configuration has the
+        irrep wfnsym (csfstring.py:74-88): per block the selected
+        configurations and their packed offsets.  None without symmetry."""
+        if self.wfnsym is None or self._orbsym is None:
+            return None
+        w = int(self.wfnsym)
+        st = self._symcache.get(w)
+        if st is not None:
+            return st
+        cs = self.confsym
+        sel, offs, nsel = [], [], []
+        c0 = 0
+        packed = 0
+        for b in self._blocks:
+            nconf = b["nconf"]
+            idx = torch.nonzero(cs[c0:c0 + nconf] == w).reshape(-1).to(torch.int32)
+            sel.append(idx.contiguous())
+            offs.append(packed)
+            nsel.append(int(idx.numel()))
+            packed += int(idx.numel()) * b["ncsf"]
+            c0 += nconf
+        idx_sym = cs[self.econf_csf_mask.long()] == w
+        st = dict(sel=sel, offs=offs, nsel=nsel, ncsf=packed, idx_sym=idx_sym,
+                  pos=torch.cumsum(idx_sym.to(torch.int64), 0) - 1)
+        self._symcache[w] = st
+        return st
+
+    @property
+    def idx_sym(self):
+        """Boolean device mask over all CSFs: those of the irrep wfnsym (the
+        idx_sym of csf_symm.py:77); None without symmetry."""
+        st = self._sym()
+        return None if st is None else st["idx_sym"]
+
+    def _c_blocks(self, with_zmat=False, packed=True):
         if with_zmat:
             for b in self._blocks:
                 if b["ncsf"] and b["nspin"] >= 2 and b["zmat"] is None:
@@ -226,30 +279,44 @@ class CSFTransformer:
             arr[i].sign = b["sign"]
             arr[i].umat = b["umat"].data_ptr() if b["umat"] is not None and b["umat"].numel() else None
             arr[i].zmat = b["zmat"].data_ptr() if b["zmat"] is not None else None
+        st = self._sym() if packed else None
+        if st is not None:
+            for i in range(len(self._blocks)):
+                arr[i].nconf = st["nsel"][i]
+                arr[i].csf_offset = st["offs"][i]
+                arr[i].conf_sel = st["sel"][i].data_ptr() if st["nsel"][i] else None
         return arr
 
     # ---- device transforms ----------------------------------------------
     def dev_det2csf(self, x):
-        """x: device (nvec, ndet) -> (nvec, ncsf), no normalisation."""
+        """x: device (nvec, ndet) -> (nvec, ncsf), no normalisation; with
+        point-group symmetry the CSF vector is the packed one (only the
+        configurations of the irrep wfnsym are formed)."""
         x = x.reshape(-1, self.ndet).contiguous()
-        out = torch.empty((x.shape[0], self._ncsf), dtype=torch.float64, device=x.device)
+        n = self.ncsf
+        out = torch.empty((x.shape[0], n), dtype=torch.float64, device=x.device)
         blocks = self._c_blocks()
-        _capi.call("csffci_det2csf", x.shape[0], ptr(x), self.ndet, ptr(out), self._ncsf,
+        _capi.call("csffci_det2csf", x.shape[0], ptr(x), self.ndet, ptr(out), n,
                    ptr(self.csd_mask), blocks, len(self._blocks), stream())
         return out
 
     def dev_csf2det(self, x):
-        """x: device (nvec, ncsf) -> (nvec, ndet), no normalisation."""
-        x = x.reshape(-1, self._ncsf).contiguous()
+        """x: device (nvec, ncsf) -> (nvec, ndet), no normalisation (packed
+        CSF vectors with point-group symmetry)."""
+        n = self.ncsf
+        x = x.reshape(-1, n).contiguous()
         out = torch.empty((x.shape[0], self.ndet), dtype=torch.float64, device=x.device)
         blocks = self._c_blocks()
-        _capi.call("csffci_csf2det", x.shape[0], ptr(x), self._ncsf, ptr(out), self.ndet, self.ndet,
+        _capi.call("csffci_csf2det", x.shape[0], ptr(x), n, ptr(out), self.ndet, self.ndet,
                    ptr(self.csd_mask), blocks, len(self._blocks), stream())
         return out
 
-    def dev_hdiag_csf(self, hdiag_det, eri4):
-        out = torch.empty(self._ncsf, dtype=torch.float64, device=device())
-        blocks = self._c_blocks(with_zmat=True)
+    def dev_hdiag_csf(self, hdiag_det, eri4, packed=False):
+        """CSF diagonal over all CSFs (as make_hdiag_csf returns it,
+        csf.py:70-144), or over the packed symmetric CSFs."""
+        st = self._sym() if packed else None
+        out = torch.empty(self._ncsf if st is None else st["ncsf"], dtype=torch.float64, device=device())
+        blocks = self._c_blocks(with_zmat=True, packed=packed)
         _capi.call("csffci_hdiag_csf", self._norb, self._neleca, self._nelecb, ptr(hdiag_det),
                    ptr(eri4), ptr(self.csd_mask), blocks, len(self._blocks), ptr(out), stream())
         return out
@@ -263,7 +330,7 @@ class CSFTransformer:
             return None
         if self._eta is None:
             g = torch.Generator(device="cpu").manual_seed(7)
-            x = torch.randn(self._ncsf, generator=g, dtype=torch.float64).to(device())
+            x = torch.randn(max(self.ncsf, 1), generator=g, dtype=torch.float64)[:self.ncsf].to(device())
             c = self.dev_csf2det(x).reshape(self.ndeta, self.ndetb)
             sym = float(torch.linalg.norm(c - c.T))
             anti = float(torch.linalg.norm(c + c.T))
@@ -290,7 +357,7 @@ class CSFTransformer:
         is_torch = isinstance(arr, torch.Tensor)
         is_list = isinstance(arr, list)
         is_tuple = isinstance(arr, tuple)
-        ncol_in = self._ncsf if reverse else self.ndet
+        ncol_in = self.ncsf if reverse else self.ndet
         if is_list or is_tuple:
             nvec = len(arr)
             is_flat = False
@@ -344,17 +411,80 @@ class CSFTransformer:
         from .csf import _pspace_transform
         return _pspace_transform(self, mat, confs)
 
+    def _pack(self, vec, idx, order, n_full):
+        if idx is None:
+            return vec
+        is_torch = isinstance(vec, torch.Tensor)
+        is_seq = isinstance(vec, (list, tuple))
+        if is_seq:
+            return type(vec)(self._pack(v, idx, order, n_full) for v in vec)
+        x = vec if is_torch else np.asarray(vec)
+        ix = idx if is_torch and x.is_cuda else (idx.cpu().numpy() if isinstance(idx, torch.Tensor) else idx)
+        if is_torch and not x.is_cuda:
+            ix = torch.as_tensor(ix)
+        if x.ndim == 1:
+            return x[ix]
+        if order.upper() == 'F':
+            return x[ix, :]
+        return x.reshape(-1, n_full)[:, ix]
+
+    def _unpack(self, vec, idx, order, n_full):
+        if idx is None:
+            return vec
+        is_torch = isinstance(vec, torch.Tensor)
+        if isinstance(vec, (list, tuple)):
+            return type(vec)(self._unpack(v, idx, order, n_full) for v in vec)
+        x = vec if is_torch else np.asarray(vec)
+        if is_torch:
+            ix = idx.to(x.device)
+            if x.ndim == 1:
+                out = torch.zeros(n_full, dtype=x.dtype, device=x.device)
+                out[ix] = x
+            elif order.upper() == 'F':
+                out = torch.zeros((n_full, x.shape[1]), dtype=x.dtype, device=x.device)
+                out[ix, :] = x
+            else:
+                out = torch.zeros((x.shape[0], n_full), dtype=x.dtype, device=x.device)
+                out[:, ix] = x
+            return out
+        ix = idx.cpu().numpy() if isinstance(idx, torch.Tensor) else idx
+        if x.ndim == 1:
+            out = np.zeros(n_full, dtype=x.dtype)
+            out[ix] = x
+        elif order.upper() == 'F':
+            out = np.zeros((n_full, x.shape[1]), dtype=x.dtype)
+            out[ix, :] = x
+        else:
+            out = np.zeros((x.shape[0], n_full), dtype=x.dtype)
+            out[:, ix] = x
+        return out
+
     def pack_csf(self, csfvec, order='C'):
-        return csfvec
+        """csfstring.py:74-79: full CSF vector(s) -> the CSFs of irrep wfnsym."""
+        return self._pack(csfvec, self.idx_sym, order, self._ncsf)
 
     def unpack_csf(self, csfvec, order='C'):
-        return csfvec
+        """csfstring.py:81-86: packed symmetric CSF vector(s) -> full, zeros
+        elsewhere."""
+        return self._unpack(csfvec, self.idx_sym, order, self._ncsf)
+
+    def _idx_sym_det(self):
+        if self.wfnsym is None or self._orbsym is None:
+            return None
+        return self.confsym[self.econf_det_mask.long()] == int(self.wfnsym)
 
     def pack_det(self, detvec, order='C'):
-        return detvec
+        """csfstring.py:88-96: determinant vector(s) -> the determinants whose
+        configuration has irrep wfnsym."""
+        if isinstance(detvec, (np.ndarray, torch.Tensor)) and tuple(detvec.shape[-2:]) == (self.ndeta, self.ndetb):
+            detvec = detvec.reshape(-1, self.ndet)
+            if detvec.shape[0] == 1:
+                detvec = detvec[0]
+        return self._pack(detvec, self._idx_sym_det(), order, self.ndet)
 
     def unpack_det(self, detvec, order='C'):
-        return detvec
+        """csfstring.py:98-103."""
+        return self._unpack(detvec, self._idx_sym_det(), order, self.ndet)
 
     # ---- properties (setting one triggers a cache update) ---------------
     @property
@@ -393,6 +523,10 @@ class CSFTransformer:
     def orbsym(self):
         return self._orbsym
 
+    @orbsym.setter
+    def orbsym(self, x):
+        self._update_symm_cache(x)
+
     @property
     def ndeta(self):
         return comb(self._norb, self._neleca)
@@ -407,7 +541,10 @@ class CSFTransformer:
 
     @property
     def ncsf(self):
-        return self._ncsf
+        """csfstring.py:205-208: the number of CSFs of irrep wfnsym when
+        point-group symmetry is set, else of all CSFs."""
+        st = self._sym()
+        return self._ncsf if st is None else st["ncsf"]
 
     def print_config(self, printer=print):
         printer('***** CSFTransformer configuration *****')
@@ -418,6 +555,41 @@ class CSFTransformer:
         printer('wfnsym = {}'.format(self.wfnsym))
         printer('ndeta, ndetb = {}, {}'.format(self.ndeta, self.ndetb))
         printer('ncsf = {}'.format(self.ncsf))
+
+
+def gen_strs_irrep(strs, orbsym):
+    """Irrep of each occupation string: the XOR of the irreps of its
+    occupied orbitals (the direct product in D2h and its subgroups, PySCF
+    irrep ids), as direct_spin1_symm._gen_strs_irrep is used at
+    csfstring.py:280-285."""
+    orbsym = torch.as_tensor(np.asarray(orbsym, dtype=np.int64), device=strs.device)
+    out = torch.zeros(strs.shape, dtype=torch.int64, device=strs.device)
+    for p in range(orbsym.numel()):
+        out ^= ((strs >> p) & 1) * orbsym[p]
+    return out
+
+
+def make_confsym(norb, neleca, nelecb, econf_det_mask, orbsym):
+    """csfstring.py:278-290: irrep of every electron configuration (all
+    determinants of a configuration share it), as a device int64 tensor
+    indexed by configuration."""
+    if np.any(np.asarray(orbsym) > 7):
+        raise NotImplementedError('High-momentum point groups in Dooh/Coov')
+    dev = econf_det_mask.device
+    na, nb = comb(norb, neleca), comb(norb, nelecb)
+    stra = torch.empty(na, dtype=torch.int64, device=dev)
+    _capi.call("csffci_gen_strings", norb, neleca, ptr(stra), stream())
+    strb = stra
+    if nelecb != neleca:
+        strb = torch.empty(nb, dtype=torch.int64, device=dev)
+        _capi.call("csffci_gen_strings", norb, nelecb, ptr(strb), stream())
+    ia = gen_strs_irrep(stra, orbsym)
+    ib = gen_strs_irrep(strb, orbsym)
+    detsym = (ia[:, None] ^ ib[None, :]).reshape(-1)
+    nconf = int(econf_det_mask.max().item()) + 1 if econf_det_mask.numel() else 0
+    confsym = torch.zeros(nconf, dtype=torch.int64, device=dev)
+    confsym[econf_det_mask.long()] = detsym
+    return confsym
 
 
 def make_econf_csf_mask(norb, neleca, nelecb, smult):

@@ -894,6 +894,12 @@ int csffci_batch_plan_create(int nprob, const csffci_batch_problem_t* probs, con
       set_error("batch_plan_create: max_space + 2*nroots = %d exceeds %d", cap, DB_CAPMAX);
       return CSFFCI_ERR_INVALID;
     }
+    for (int b = 0; b < q.nblocks; ++b)
+      if (q.blocks[b].conf_sel != nullptr) {
+        delete P;
+        set_error("batch_plan_create: problem %d: point-group-restricted CSF blocks are not supported", i);
+        return CSFFCI_ERR_INVALID;
+      }
     P->blocks[i].assign(q.blocks, q.blocks + q.nblocks);
     DBProb& d = P->prob[i];
     memset(&d, 0, sizeof(d));

@@ -20,6 +20,7 @@ struct BlockGemmArgs {
   const uint32_t* mask;
   const double* umat;
   int64_t csd_off, csf_off, nconf;
+  const int32_t* conf_sel;  // selected configurations (point-group symmetry) or NULL
   int ndet, ncsf;
   int nvec;
   double sign;
@@ -57,7 +58,8 @@ __global__ void __launch_bounds__(256) k_block_gemm(BlockGemmArgs g) {
         if (m < M && k0 + kk < K) {
           int64_t vec = m / g.nconf, conf = m - vec * g.nconf;
           if (MODE == MODE_DET2CSF) {
-            uint32_t d = g.mask[g.csd_off + conf * g.ndet + k0 + kk];
+            const int64_t cf = g.conf_sel ? g.conf_sel[conf] : conf;
+            uint32_t d = g.mask[g.csd_off + cf * g.ndet + k0 + kk];
             v = g.x[vec * g.ldx + d];
           } else {
             v = g.x[vec * g.ldx + g.csf_off + conf * g.ncsf + k0 + kk];
@@ -107,7 +109,8 @@ __global__ void __launch_bounds__(256) k_block_gemm(BlockGemmArgs g) {
         if (MODE == MODE_DET2CSF) {
           g.y[vec * g.ldy + g.csf_off + conf * g.ncsf + n] = v;
         } else {
-          uint32_t d = g.mask[g.csd_off + conf * g.ndet + n];
+          const int64_t cf = g.conf_sel ? g.conf_sel[conf] : conf;
+          uint32_t d = g.mask[g.csd_off + cf * g.ndet + n];
           g.y[vec * g.ldy + d] = v;
         }
       }
@@ -141,6 +144,7 @@ static int run_blocks(int nvec, const double* x, int64_t ldx, double* y, int64_t
     g.csd_off = B.csd_offset;
     g.csf_off = B.csf_offset;
     g.nconf = B.nconf;
+    g.conf_sel = B.conf_sel;
     g.ndet = B.ndet;
     g.ncsf = B.ncsf;
     g.nvec = nvec;
@@ -172,6 +176,7 @@ struct HdiagCsfArgs {
   const double* zmat;
   double* out;
   int64_t csd_off, csf_off, nconf, sconf;
+  const int32_t* conf_sel;
   int ndet, ncsf, nspin, npair, norb, npair_orb;
 };
 
@@ -179,8 +184,9 @@ __global__ void k_hdiag_csf(HdiagCsfArgs g) {
   const int64_t n = g.nconf * g.ncsf;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t conf = i / g.ncsf;
-    int k = (int)(i - conf * g.ncsf);
+    const int64_t ic = i / g.ncsf;  // position in the (packed) CSF vector
+    const int k = (int)(i - ic * g.ncsf);
+    const int64_t conf = g.conf_sel ? g.conf_sel[ic] : ic;  // configuration within the block
     double acc = 0.0;
     const uint32_t* m = g.mask + g.csd_off + conf * g.ndet;
     for (int x = 0; x < g.ndet; ++x) {
@@ -205,7 +211,7 @@ __global__ void k_hdiag_csf(HdiagCsfArgs g) {
           acc = fma(g.eri[(int64_t)pq * g.npair_orb + pq], g.zmat[(int64_t)ab * g.ncsf + k], acc);
         }
     }
-    g.out[g.csf_off + conf * g.ncsf + k] = acc;
+    g.out[g.csf_off + ic * g.ncsf + k] = acc;
   }
 }
 
@@ -233,7 +239,7 @@ int csffci_csf2det(int nvec, const double* x_csf, int64_t ld_csf, double* x_det,
   // simplicity of the contract) start from zero
   bool full = true;
   for (int b = 0; b < nblock; ++b)
-    if (blocks[b].ncsf == 0 && blocks[b].nconf > 0) full = false;
+    if ((blocks[b].ncsf == 0 && blocks[b].nconf > 0) || blocks[b].conf_sel != nullptr) full = false;
   if (!full) {
     k_zero_rows<<<grid_for((int64_t)nvec * ndet, 256, 148 * 16), 256, 0, stream>>>(x_det, ld_det,
                                                                                      nvec, ndet);
@@ -264,6 +270,7 @@ int csffci_hdiag_csf(int norb, int neleca, int nelecb, const double* hdiag_det, 
     g.csd_off = B.csd_offset;
     g.csf_off = B.csf_offset;
     g.nconf = B.nconf;
+    g.conf_sel = B.conf_sel;
     g.sconf = (int64_t)host_binom(norb - B.npair, B.nspin);
     g.ndet = B.ndet;
     g.ncsf = B.ncsf;

@@ -105,6 +105,61 @@ def small_case(tag, norb, nelec, smult, rank, nroots=1, full=True):
     print("%s: ndet=%d ncsf=%d  %.1fs -> %s" % (tag, ndet, T.ncsf, time.time() - t0, path))
 
 
+def symmetric_integrals(norb, rank, orbsym, seed=0):
+    """The seeded integrals with every element that breaks the point group
+    of orbsym zeroed: h1[p,q] = 0 unless irrep(p) = irrep(q); (pq|rs) = 0
+    unless irrep(p)^irrep(q)^irrep(r)^irrep(s) = 0 (D2h subgroup ids)."""
+    h1, eri = seeded_integrals(norb, rank, seed)
+    o = np.asarray(orbsym)
+    h1 = h1 * (o[:, None] == o[None, :])
+    eri = eri * ((o[:, None, None, None] ^ o[None, :, None, None] ^ o[None, None, :, None]
+                  ^ o[None, None, None, :]) == 0)
+    return h1, eri
+
+
+def symm_case(tag, norb, nelec, smult, rank, orbsym, wfnsym, nroots=1):
+    """The reference's point-group-symmetric solver (csf_symm.FCISolver) and
+    symmetric transformer on symmetry-adapted integrals: configuration
+    irreps, packed det<->CSF transforms, the symmetric p-space and the
+    energies of irrep wfnsym."""
+    from pyscf.csf_fci import csf_symm
+    t0 = time.time()
+    na, nb = nelec
+    h1, eri = symmetric_integrals(norb, rank, orbsym)
+    out = dict(norb=norb, neleca=na, nelecb=nb, smult=smult, nroots=nroots, h1=h1, eri=eri,
+               orbsym=np.asarray(orbsym), wfnsym=wfnsym)
+    T = CSFTransformer(norb, na, nb, smult, orbsym=np.asarray(orbsym), wfnsym=wfnsym)
+    out["confsym"] = np.asarray(T.confsym)
+    idx_sym = T.confsym[T.econf_csf_mask] == wfnsym
+    out["idx_sym"] = idx_sym
+    rng = np.random.default_rng(2)
+    ci = rng.normal(size=T.ndet)
+    out["ci_rand"] = ci
+    out["det2csf_sym"] = T.vec_det2csf(ci, normalize=False)
+    x = rng.normal(size=T.ncsf)
+    out["csf_sym_rand"] = x
+    out["csf2det_sym"] = T.vec_csf2det(x, normalize=False)
+    sol = csf_symm.FCISolver(None, smult=smult)
+    sol.nroots = nroots
+    sol.orbsym = np.asarray(orbsym)
+    sol.wfnsym = wfnsym
+    sol.norb, sol.nelec = norb, nelec
+    sol.check_transformer_cache()
+    npsp = min(60, T.ncsf)
+    addr, h0 = sol.pspace(h1, eri, norb, nelec, npsp=npsp)
+    order = np.argsort(addr)
+    out["pspace_addr"] = np.asarray(addr)[order]
+    out["pspace_h0"] = np.asarray(h0)[np.ix_(order, order)]
+    sol.conv_tol = 1e-12
+    e, c = sol.kernel(h1, eri, norb, nelec, orbsym=np.asarray(orbsym), wfnsym=wfnsym)
+    out["energies"] = np.atleast_1d(e)
+    cs = [c] if nroots == 1 else list(c)
+    out["ci_roots"] = np.array([np.asarray(ci_).ravel() for ci_ in cs])
+    path = os.path.join(HERE, "%s.npz" % tag)
+    np.savez_compressed(path, **out)
+    print("%s: ndet=%d ncsf_sym=%d  %.1fs -> %s  E=%s" % (tag, T.ndet, T.ncsf, time.time() - t0, path, e))
+
+
 def c1_case():
     """norb=12 (6,6) singlet, 3 roots: bit-exact hashes of the integer maps
     and fingerprints of the floating results (the full vectors are too big
@@ -158,5 +213,8 @@ if __name__ == "__main__":
     small_case("norb4_4e4e_s0", 4, (4, 4), 1, 6, full=False)
     small_case("norb5_1e0e_s12", 5, (1, 0), 2, 6, full=False)
     small_case("norb7_4e3e_s32", 7, (4, 3), 4, 10, nroots=2)
+    symm_case("symm_norb8_4e4e_s0_w2", 8, (4, 4), 1, 16, [0, 2, 0, 3, 1, 0, 2, 3], 2, nroots=2)
+    symm_case("symm_norb7_4e3e_s12_w1", 7, (4, 3), 2, 12, [0, 1, 0, 1, 3, 2, 0], 1, nroots=2)
+    symm_case("symm_norb6_3e3e_s1_w3", 6, (3, 3), 3, 10, [0, 1, 2, 3, 0, 1], 3, nroots=1)
     if args.c1:
         c1_case()

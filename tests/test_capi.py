@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol():
 def test_struct_layouts():
     from pyscf_forge_b200 import _capi
     assert ctypes.sizeof(_capi.LinkEntry) == 8
-    assert ctypes.sizeof(_capi.Block) == 64
+    assert ctypes.sizeof(_capi.Block) == 72
 
 
 def test_struct_layouts_match_header(tmp_path):
