@@ -246,6 +246,17 @@ int csffci_contract_1e(int norb, int neleca, int nelecb, const double* h1a,
                        const csffci_link_t* link_b, const double* ci, double* sigma,
                        cudaStream_t stream);
 
+/* ---- spin ladder operators (contract_sladder,
+ *      pyscf/csf_fci/spin_op.py:22-68) ------------------------------------ */
+
+/* out = S- ci (op = -1: an alpha electron becomes beta) or S+ ci (op = +1)
+ * for a determinant vector of (neleca, nelecb) electrons; out is the
+ * (C(norb, neleca+op), C(norb, nelecb-op)) vector, fully overwritten, with
+ * the sign convention of the reference's spin_op.py.  mup/mdown and
+ * <S^2> (spin_square) are built on it. */
+int csffci_spin_ladder(int norb, int neleca, int nelecb, int op, const double* ci, double* out,
+                       cudaStream_t stream);
+
 /* ---- density matrices (direct_spin1.make_rdm12/trans_rdm12, inherited at
  *      csf.py:557; reference twin fci_rdm_gas_plan_make_rdm12s,
  *      fci_rdm_gas.c:2207-2243, assembled as fci_gas.py:724-733) --------- */

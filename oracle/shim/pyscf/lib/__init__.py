@@ -62,3 +62,14 @@ def fp(a):
 
 def davidson1(*a, **k):
     raise NotImplementedError("the stand-in drives Davidson through FCISolver.eig")
+
+
+def take_2d(a, idx, idy):
+    """a[idx][:, idy] as a new array (role of lib.take_2d)."""
+    return np.asarray(a)[np.ix_(np.asarray(idx), np.asarray(idy))].copy()
+
+
+def takebak_2d(out, a, idx, idy):
+    """out[idx[:, None], idy] += a (role of lib.takebak_2d)."""
+    out[np.ix_(np.asarray(idx), np.asarray(idy))] += a
+    return out

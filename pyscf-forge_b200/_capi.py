@@ -157,6 +157,7 @@ _SIGS = {
     "csffci_dots_batch": ([_i, _p, _p, _p, _sz, _p], _i),
     "csffci_combine_batch": ([_i, _p, _p, _sz, _p], _i),
     "csffci_precond_batch": ([_i, _p, _p, _sz, _p], _i),
+    "csffci_spin_ladder": ([_i, _i, _i, _i, _p, _p, _p], _i),
     "csffci_batch_plan_create": ([_i, _p, _p, ctypes.POINTER(_p), ctypes.POINTER(_sz)], _i),
     "csffci_batch_plan_bind": ([_p, _p, _sz, _p], _i),
     "csffci_batch_plan_run": ([_p, _p, ctypes.POINTER(_i)], _i),

@@ -1,5 +1,5 @@
 """CSF-basis FCI (pyscf/csf_fci/__init__.py:1-12)."""
-from . import csf, csfstring, csdstring, csf_symm  # noqa: F401
+from . import csf, csfstring, csdstring, csf_symm, spin_op  # noqa: F401
 from .csf import FCISolver
 from .csfstring import CSFTransformer
 

@@ -369,6 +369,14 @@ class FCIBase:
     def energy(self, h1e, eri, fcivec, norb, nelec, link_index=None):
         return direct_spin1.energy(h1e, eri, fcivec, norb, nelec)
 
+    def spin_square(self, fcivec, norb, nelec):
+        """(<S^2>, 2S+1) per vector (fci.spin_op.spin_square0 semantics)."""
+        from .spin_op import spin_square
+        if isinstance(fcivec, (list, tuple)):
+            res = [spin_square(c, norb, nelec) for c in fcivec]
+            return [r[0] for r in res], [r[1] for r in res]
+        return spin_square(fcivec, norb, nelec)
+
 
 class CSFFCISolver:
     """csf.py:499-555."""

@@ -160,6 +160,38 @@ def symm_case(tag, norb, nelec, smult, rank, orbsym, wfnsym, nroots=1):
     print("%s: ndet=%d ncsf_sym=%d  %.1fs -> %s  E=%s" % (tag, T.ndet, T.ncsf, time.time() - t0, path, e))
 
 
+def spin_case():
+    """The reference's spin ladder operators (csf_fci/spin_op.py) on the
+    triplet solution of norb6_4e2e_s1 (M_S = 1): mdown to M_S = 0 and -1,
+    mup back, and S+/S- of a random M_S = 0 vector."""
+    from pyscf.csf_fci import spin_op
+    g = np.load(os.path.join(HERE, "norb6_4e2e_s1.npz"))
+    norb, smult = 6, 3
+    c = g["ci_roots"][0].reshape(R.num_strings(6, 4), R.num_strings(6, 2))
+    out = dict(norb=norb, smult=smult, ci_high=c)
+    out["mdown_33"] = spin_op.mdown(c, norb, (3, 3), smult)
+    out["mdown_24"] = spin_op.mdown(c, norb, (2, 4), smult)
+    out["mup_from_33"] = spin_op.mup(out["mdown_33"], norb, (3, 3), smult)
+    # the lowered vector is an eigenvector of H with the same energy
+    h2e = R.absorb_h1e(g["h1"], g["eri"], norb, (3, 3), 0.5)
+    v = out["mdown_33"]
+    hv = gasref.contract_2e(h2e, v, norb, (3, 3))
+    e = float(g["energies"][0])
+    assert np.linalg.norm(hv - e * v) < 1e-8, np.linalg.norm(hv - e * v)
+    rng = np.random.default_rng(5)
+    x = rng.normal(size=(R.num_strings(6, 3), R.num_strings(6, 3)))
+    out["x_33"] = x
+    out["sup_x"] = spin_op.contract_sup(x, norb, (3, 3))
+    out["sdown_x"] = spin_op.contract_sdown(x, norb, (3, 3))
+    y = rng.normal(size=(R.num_strings(7, 4), R.num_strings(7, 2)))
+    out["y_42_n7"] = y
+    out["sup_y"] = spin_op.contract_sup(y, 7, (4, 2))
+    out["sdown_y"] = spin_op.contract_sdown(y, 7, (4, 2))
+    path = os.path.join(HERE, "spin_ladder_norb6.npz")
+    np.savez_compressed(path, **out)
+    print("spin ladder -> %s" % path)
+
+
 def c1_case():
     """norb=12 (6,6) singlet, 3 roots: bit-exact hashes of the integer maps
     and fingerprints of the floating results (the full vectors are too big
@@ -216,5 +248,6 @@ if __name__ == "__main__":
     symm_case("symm_norb8_4e4e_s0_w2", 8, (4, 4), 1, 16, [0, 2, 0, 3, 1, 0, 2, 3], 2, nroots=2)
     symm_case("symm_norb7_4e3e_s12_w1", 7, (4, 3), 2, 12, [0, 1, 0, 1, 3, 2, 0], 1, nroots=2)
     symm_case("symm_norb6_3e3e_s1_w3", 6, (3, 3), 3, 10, [0, 1, 2, 3, 0, 1], 3, nroots=1)
+    spin_case()
     if args.c1:
         c1_case()
