@@ -269,6 +269,17 @@ int csffci_rdm12(int norb, int neleca, int nelecb, const csffci_link_t* link_a,
                  double* dm1, double* dm2, void* work, size_t work_bytes,
                  cudaStream_t stream);
 
+/* Spin-resolved RDMs (make_rdm12s / trans_rdm12s, inherited at csf.py:557;
+ * reference twin fci_rdm_gas_plan_make_rdm12s, fci_rdm_gas.c:2207-2243):
+ * dm1s[p][q] = <bra|q+ p|ket> per spin, dm2aa[p][q][r][s] = <p+_a r+_a s_a q_a>,
+ * dm2ab = <p+_a r+_b s_b q_a>, dm2bb = <p+_b r+_b s_b q_b>.  The three 2-RDM
+ * blocks are all given or all NULL (1-RDMs only). */
+size_t csffci_rdm12s_workspace(int norb, int neleca, int nelecb);
+int csffci_rdm12s(int norb, int neleca, int nelecb, const csffci_link_t* link_a,
+                  const csffci_link_t* link_b, const double* bra, const double* ket, double* dm1a,
+                  double* dm1b, double* dm2aa, double* dm2ab, double* dm2bb, void* work,
+                  size_t work_bytes, cudaStream_t stream);
+
 /* ---- Davidson update (role of pyscf lib.davidson1 via fci.eig at
  *      csf.py:487-490) --------------------------------------------------- */
 

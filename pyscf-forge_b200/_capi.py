@@ -145,6 +145,8 @@ _SIGS = {
     "csffci_contract_1e": ([_i, _i, _i, _p, _p, _p, _p, _p, _p, _p], _i),
     "csffci_rdm12_workspace": ([_i, _i, _i], _sz),
     "csffci_rdm12": ([_i, _i, _i, _p, _p, _p, _p, _p, _p, _p, _sz, _p], _i),
+    "csffci_rdm12s_workspace": ([_i, _i, _i], _sz),
+    "csffci_rdm12s": ([_i, _i, _i] + [_p] * 10 + [_sz, _p], _i),
     "csffci_gram_workspace": ([_i, _i, _i64], _sz),
     "csffci_gram": ([_i, _p, _i64, _i, _p, _i64, _i64, _p, _p, _sz, _p], _i),
     "csffci_combine": ([_i, _p, _i64, _d, _i, _p, _i64, _p, _i64, _p], _i),

@@ -363,6 +363,18 @@ class FCIBase:
     def trans_rdm1(self, cibra, ciket, norb, nelec, link_index=None):
         return direct_spin1.trans_rdm1(cibra, ciket, norb, nelec)
 
+    def make_rdm1s(self, fcivec, norb, nelec, link_index=None):
+        return direct_spin1.make_rdm1s(fcivec, norb, nelec)
+
+    def make_rdm12s(self, fcivec, norb, nelec, link_index=None, reorder=True):
+        return direct_spin1.make_rdm12s(fcivec, norb, nelec)
+
+    def trans_rdm1s(self, cibra, ciket, norb, nelec, link_index=None):
+        return direct_spin1.trans_rdm1s(cibra, ciket, norb, nelec)
+
+    def trans_rdm12s(self, cibra, ciket, norb, nelec, link_index=None, reorder=True):
+        return direct_spin1.trans_rdm12s(cibra, ciket, norb, nelec)
+
     def trans_rdm12(self, cibra, ciket, norb, nelec, link_index=None, reorder=True):
         return direct_spin1.trans_rdm12(cibra, ciket, norb, nelec)
 

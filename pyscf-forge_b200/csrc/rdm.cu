@@ -155,6 +155,24 @@ __global__ void k_rdm_assemble(int norb, const double* __restrict__ G, const dou
   }
 }
 
+// spin-resolved assembly: dm2[p][q][r][s] = G[(qp)][(rs)] - d_qr d1[p][s]
+// (same-spin blocks) or G[(qp)][(rs)] (alpha-beta block, d1 == NULL)
+__global__ void k_rdm_assemble_s(int norb, const double* __restrict__ G, const double* __restrict__ d1,
+                                 double* dm2) {
+  const int n = norb, n2 = n * n;
+  long long tot = (long long)n2 * n2;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    int p = (int)(t / ((long long)n * n2));
+    int q = (int)((t / n2) % n);
+    int r = (int)((t / n) % n);
+    int s = (int)(t % n);
+    double v = G[(long long)(q * n + p) * n2 + r * n + s];
+    if (d1 && q == r) v -= d1[p * n + s];
+    dm2[t] = v;
+  }
+}
+
 __global__ void k_transpose_small(int n, const double* in, double* out) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n * n; t += gridDim.x * blockDim.x) {
     int i = t / n, j = t - i * n;
@@ -246,6 +264,102 @@ int csffci_rdm12(int norb, int neleca, int nelecb, const csffci_link_t* link_a,
   if (dm2) {
     k_rdm_assemble<<<grid_for((long long)n2 * n2, 256, 148 * 8), 256, 0, stream>>>(norb, G, dm1, dm2);
     return check_launch("rdm2 assemble");
+  }
+  return CSFFCI_OK;
+}
+
+static long long rdm12s_slab(long long ndet) {
+  long long S = ndet < (1ll << 17) ? ndet : (1ll << 17);
+  return S < 1 ? 1 : S;
+}
+
+size_t csffci_rdm12s_workspace(int norb, int neleca, int nelecb) {
+  long long ndet = (long long)(host_binom(norb, neleca) * host_binom(norb, nelecb));
+  long long n2 = (long long)norb * norb;
+  long long S = rdm12s_slab(ndet);
+  size_t t = (size_t)(4 * S * n2) * sizeof(double);
+  size_t g = (size_t)(3 * n2 * n2 + 4 * n2) * sizeof(double);
+  size_t part = gram_workspace((int)n2, (int)n2, S);
+  size_t part1 = gram_workspace(1, (int)n2, S);
+  return t + g + (part > part1 ? part : part1) + 1024;
+}
+
+int csffci_rdm12s(int norb, int neleca, int nelecb, const csffci_link_t* link_a,
+                  const csffci_link_t* link_b, const double* bra, const double* ket, double* dm1a,
+                  double* dm1b, double* dm2aa, double* dm2ab, double* dm2bb, void* work,
+                  size_t work_bytes, cudaStream_t stream) {
+  CSF_REQUIRE(norb >= 1 && norb <= 22, "rdm12s: norb=%d outside [1,22]", norb);
+  CSF_REQUIRE(dm1a && dm1b && bra && ket, "rdm12s: NULL argument");
+  CSF_REQUIRE((dm2aa == nullptr) == (dm2ab == nullptr) && (dm2ab == nullptr) == (dm2bb == nullptr),
+              "rdm12s: the three 2-RDM blocks are all given or all NULL");
+  long long Na = (long long)host_binom(norb, neleca), Nb = (long long)host_binom(norb, nelecb);
+  long long ndet = Na * Nb;
+  int n2 = norb * norb;
+  int nla = neleca * (norb - neleca + 1), nlb = nelecb * (norb - nelecb + 1);
+  size_t need = csffci_rdm12s_workspace(norb, neleca, nelecb);
+  if (work == nullptr || work_bytes < need) {
+    set_error("rdm12s: workspace of %zu bytes < %zu required", work_bytes, need);
+    return CSFFCI_ERR_MEMORY;
+  }
+  const long long S = rdm12s_slab(ndet);
+  double* Tka = (double*)work;  // <J|E^alpha_pq|ket>
+  double* Tkb = Tka + (size_t)S * n2;
+  double* Tba = Tkb + (size_t)S * n2;  // the same for bra
+  double* Tbb = Tba + (size_t)S * n2;
+  double* Gaa = Tbb + (size_t)S * n2;
+  double* Gab = Gaa + (size_t)n2 * n2;
+  double* Gbb = Gab + (size_t)n2 * n2;
+  double* d1at = Gbb + (size_t)n2 * n2;
+  double* d1bt = d1at + n2;
+  double* part = d1bt + 2 * (size_t)n2;
+  const bool same = (bra == ket);
+  const bool two = dm2aa != nullptr;
+  int st;
+  for (long long J0 = 0; J0 < ndet; J0 += S) {
+    const long long s = (ndet - J0 < S) ? ndet - J0 : S;
+    const int accumulate = J0 > 0;
+    for (int which = 0; which < (same ? 1 : 2); ++which) {
+      const double* c = which == 0 ? ket : bra;
+      double* Ta = which == 0 ? Tka : Tba;
+      double* Tb = which == 0 ? Tkb : Tbb;
+      k_zero<<<grid_for(s * n2, 256, 148 * 16), 256, 0, stream>>>(Ta, s * n2);
+      if ((st = check_launch("rdm12s T zero"))) return st;
+      k_zero<<<grid_for(s * n2, 256, 148 * 16), 256, 0, stream>>>(Tb, s * n2);
+      if ((st = check_launch("rdm12s T zero"))) return st;
+      if (nla > 0) {
+        k_tslab_links<<<grid_for(s * nla, 256, 148 * 16), 256, 0, stream>>>(
+            norb, Nb, nla, nlb, link_a, link_b, c, J0, s, 0, Ta);
+        if ((st = check_launch("rdm12s T alpha"))) return st;
+      }
+      if (nlb > 0) {
+        k_tslab_links<<<grid_for(s * nlb, 256, 148 * 16), 256, 0, stream>>>(
+            norb, Nb, nla, nlb, link_a, link_b, c, J0, s, 1, Tb);
+        if ((st = check_launch("rdm12s T beta"))) return st;
+      }
+    }
+    const double* BA = same ? Tka : Tba;
+    const double* BB = same ? Tkb : Tbb;
+    if ((st = gram_run(1, bra + J0, s, n2, Tka, s, s, d1at, accumulate, part, stream))) return st;
+    if ((st = gram_run(1, bra + J0, s, n2, Tkb, s, s, d1bt, accumulate, part, stream))) return st;
+    if (two) {
+      if ((st = gram_run(n2, BA, s, n2, Tka, s, s, Gaa, accumulate, part, stream))) return st;
+      if ((st = gram_run(n2, BA, s, n2, Tkb, s, s, Gab, accumulate, part, stream))) return st;
+      if ((st = gram_run(n2, BB, s, n2, Tkb, s, s, Gbb, accumulate, part, stream))) return st;
+    }
+  }
+  k_transpose_small<<<grid_for(n2, 256), 256, 0, stream>>>(norb, d1at, dm1a);
+  if ((st = check_launch("rdm1a transpose"))) return st;
+  k_transpose_small<<<grid_for(n2, 256), 256, 0, stream>>>(norb, d1bt, dm1b);
+  if ((st = check_launch("rdm1b transpose"))) return st;
+  if (two) {
+    const int g = grid_for((long long)n2 * n2, 256, 148 * 8);
+    // same-spin: <p+ r+ s q> = <E_pq E_rs> - d_qr <p+ s> = ... - d_qr dm1[s][p]
+    k_rdm_assemble_s<<<g, 256, 0, stream>>>(norb, Gaa, d1at, dm2aa);
+    if ((st = check_launch("rdm2aa assemble"))) return st;
+    k_rdm_assemble_s<<<g, 256, 0, stream>>>(norb, Gab, nullptr, dm2ab);
+    if ((st = check_launch("rdm2ab assemble"))) return st;
+    k_rdm_assemble_s<<<g, 256, 0, stream>>>(norb, Gbb, d1bt, dm2bb);
+    return check_launch("rdm2bb assemble");
   }
   return CSFFCI_OK;
 }

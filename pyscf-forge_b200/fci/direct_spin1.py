@@ -151,6 +151,27 @@ def dev_rdm12(bra, ket, norb, nelec, with_dm2=True):
     return dm1, dm2
 
 
+def dev_rdm12s(bra, ket, norb, nelec, with_dm2=True):
+    """Spin-resolved RDMs on the device: ((dm1a, dm1b), (dm2aa, dm2ab,
+    dm2bb)) with dm1s[p,q] = <q+ p>, dm2ab[p,q,r,s] = <p+_a r+_b s_b q_a>
+    (conventions of fci_gas.h:260-268; reference twin
+    fci_rdm_gas_plan_make_rdm12s, fci_rdm_gas.c:2207-2243)."""
+    na, nb = nelec
+    la = dev_link_table(norb, na)
+    lb = dev_link_table(norb, nb)
+    dev = device()
+    d1 = [torch.empty((norb, norb), dtype=torch.float64, device=dev) for _ in range(2)]
+    d2 = [torch.empty((norb,) * 4, dtype=torch.float64, device=dev) for _ in range(3)] if with_dm2 \
+        else [None, None, None]
+    nbytes = _capi.query("csffci_rdm12s_workspace", norb, na, nb)
+    ws = workspace("rdm12s", nbytes)
+    bra = bra.contiguous()
+    ket = bra if ket is None else ket.contiguous()
+    _capi.call("csffci_rdm12s", norb, na, nb, ptr(la), ptr(lb), ptr(bra), ptr(ket), ptr(d1[0]), ptr(d1[1]),
+               ptr(d2[0]), ptr(d2[1]), ptr(d2[2]), ptr(ws), nbytes, stream())
+    return tuple(d1), tuple(d2)
+
+
 # ---------------------------------------------------------------------------
 # PySCF-style functions (numpy in/out, or torch when given torch)
 # ---------------------------------------------------------------------------
@@ -215,6 +236,33 @@ def trans_rdm12(cibra, ciket, norb, nelec, link_index=None, reorder=True):
     nelec = _unpack_nelec(nelec)
     dm1, dm2 = dev_rdm12(to_dev(cibra).reshape(-1), to_dev(ciket).reshape(-1), norb, nelec)
     return like_input(dm1, cibra), like_input(dm2, cibra)
+
+
+def make_rdm1s(fcivec, norb, nelec, link_index=None):
+    """(dm1a, dm1b) (direct_spin1.make_rdm1s, inherited at csf.py:557)."""
+    nelec = _unpack_nelec(nelec)
+    (d1a, d1b), _ = dev_rdm12s(to_dev(fcivec).reshape(-1), None, norb, nelec, with_dm2=False)
+    return like_input(d1a, fcivec), like_input(d1b, fcivec)
+
+
+def make_rdm12s(fcivec, norb, nelec, link_index=None, reorder=True):
+    """((dm1a, dm1b), (dm2aa, dm2ab, dm2bb)) (direct_spin1.make_rdm12s)."""
+    nelec = _unpack_nelec(nelec)
+    d1, d2 = dev_rdm12s(to_dev(fcivec).reshape(-1), None, norb, nelec)
+    return tuple(like_input(x, fcivec) for x in d1), tuple(like_input(x, fcivec) for x in d2)
+
+
+def trans_rdm1s(cibra, ciket, norb, nelec, link_index=None):
+    nelec = _unpack_nelec(nelec)
+    (d1a, d1b), _ = dev_rdm12s(to_dev(cibra).reshape(-1), to_dev(ciket).reshape(-1), norb, nelec,
+                               with_dm2=False)
+    return like_input(d1a, cibra), like_input(d1b, cibra)
+
+
+def trans_rdm12s(cibra, ciket, norb, nelec, link_index=None, reorder=True):
+    nelec = _unpack_nelec(nelec)
+    d1, d2 = dev_rdm12s(to_dev(cibra).reshape(-1), to_dev(ciket).reshape(-1), norb, nelec)
+    return tuple(like_input(x, cibra) for x in d1), tuple(like_input(x, cibra) for x in d2)
 
 
 def energy(h1e, eri, fcivec, norb, nelec, link_index=None):

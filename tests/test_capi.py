@@ -68,3 +68,19 @@ def test_struct_layouts_match_header(tmp_path):
         assert int(out[cname]) == ctypes.sizeof(py), cname
         for f in py._fields_:
             assert int(out[cname + "." + f[0]]) == getattr(py, f[0]).offset, (cname, f[0])
+
+
+def test_binding_argument_counts_match_header():
+    """Every ctypes signature has as many arguments as the header's
+    declaration (a miscounted binding would shift every later argument)."""
+    from pyscf_forge_b200 import _capi
+    decl = {}
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        txt = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        for name, params in re.findall(r"\b(csffci_\w+)\s*\(([^;{]*?)\)\s*;", txt, flags=re.S):
+            params = params.strip()
+            decl[name] = 0 if params in ("", "void") else params.count(",") + 1
+    assert decl
+    for name, (args, _) in _capi._SIGS.items():
+        assert name in decl, name
+        assert len(args) == decl[name], (name, len(args), decl[name])

@@ -72,3 +72,14 @@ def test_eri_layouts():
     e8 = e4[np.tril_indices(15)]
     np.testing.assert_allclose(eri_pair_matrix(e8, 5), e4)
     np.testing.assert_allclose(eri_pair_matrix(e4, 5), e4)
+
+
+def test_state_weights_validation():
+    """State weights: non-empty, finite, non-negative, summing to one
+    (the checks of pyscf/mcscf/addons_gas.py:103-114)."""
+    import pytest
+    from pyscf_forge_b200.state_average import validate_state_weights
+    assert list(validate_state_weights([0.25, 0.75])) == [0.25, 0.75]
+    for bad in ([], [[0.5, 0.5]], [0.5, float("nan")], [1.5, -0.5], [0.5, 0.4]):
+        with pytest.raises(ValueError):
+            validate_state_weights(bad)
