@@ -37,8 +37,10 @@ bool sigma_rr_supported(int norb) { return norb >= 4 && norb <= 16; }
 // Tile shapes (rows per warp, n-tiles of 8 columns): 16-row warps halve
 // the B-fragment traffic but need 2*KS + 4*NT doubles of registers per lane;
 // with 9 warps (norb 15,16) an SMSP holds 3 warps, i.e. at most 168
-// registers, so those sizes have no (16, 4) instance.  The default is
-// (16, 4) up to norb 14 and (8, 4) above; CSFFCI_SIGMA_VARIANT overrides it
+// registers, so those sizes have no (16, 4) instance.  The defaults are the
+// fastest shapes measured on B200 for one singlet/doublet problem: (16, 2)
+// up to norb 10, (8, 2) for 11-12, (8, 4) from 13 (the two-n-tile shapes
+// run 2-3 CTAs per SM at small norb); CSFFCI_SIGMA_VARIANT overrides them
 // and the batched solver's autotuner picks per orbital count.
 static const int kVariantShape[RR_NVARIANT][2] = {{16, 4}, {8, 4}, {16, 2}, {8, 2}};
 
@@ -50,7 +52,7 @@ int rr_default_variant(int norb) {
     const int v = atoi(env);
     if (rr_variant_valid(norb, v)) return v;
   }
-  return norb >= 15 ? 1 : 0;
+  return norb <= 10 ? 2 : norb <= 12 ? 3 : 1;
 }
 
 // fill the bookkeeping fields of the jobs; returns the largest Nb, nla, nlb
