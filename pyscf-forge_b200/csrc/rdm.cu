@@ -9,6 +9,7 @@
 // space is processed in slabs that fit the caller's workspace, so D(pq,J)
 // is never materialised for the whole space.
 #include "common.cuh"
+#include "profile.cuh"
 
 namespace csffci {
 
@@ -104,39 +105,239 @@ int gram_run(int nx, const double* x, int64_t ldx, int ny, const double* y, int6
 }
 
 // ---------------------------------------------------------------------------
-// T slab: T[pq][j] for determinants J = J0 + j, j < S, pq = p*norb + q
+// FP64 tensor-core Gram for the RDM contraction G = X Y^T (nx, ny ~ norb^2,
+// K = determinants of a slab): 64x64 tiles, 8 warps of 32x16 (m8n8k4 DMMA),
+// K staged through shared memory in 16-wide chunks (double-buffered
+// cp.async), split-K partials reduced in a fixed order.  With sym (X == Y)
+// only the tiles on and above the diagonal are formed and the reduction
+// mirrors the rest.
 // ---------------------------------------------------------------------------
-__global__ void k_zero(double* T, long long n) {
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-       t += (long long)gridDim.x * blockDim.x)
-    T[t] = 0.0;
+constexpr int GD_T = 64, GD_KC = 16, GD_LD = 20;  // LD = 4 (mod 16): conflict-free fragment loads
+
+__device__ __forceinline__ void gd_dmma(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
 }
 
-__global__ void k_tslab_links(int norb, long long Nb, int nla, int nlb,
-                              const csffci_link_t* __restrict__ la,
-                              const csffci_link_t* __restrict__ lb, const double* __restrict__ c,
-                              long long J0, long long S, int spin, double* T) {
-  const int nl = spin == 0 ? nla : nlb;
-  long long tot = S * nl;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
-       t += (long long)gridDim.x * blockDim.x) {
-    long long j = t % S;  // consecutive threads -> consecutive determinants
-    int l = (int)(t / S);
-    long long J = J0 + j;
-    long long ja = J / Nb, jb = J - ja * Nb;
-    csffci_link_t e;
-    double v;
-    if (spin == 0) {
-      e = la[ja * nla + l];
-      v = e.sign * c[(long long)e.addr * Nb + jb];
-    } else {
-      e = lb[jb * nlb + l];
-      v = e.sign * c[ja * Nb + e.addr];
-    }
-    int a = e.op & 0xff, i = e.op >> 8;
-    // <J|E_ia|I> = sign for E_ai J = sign I
-    T[(long long)(i * norb + a) * S + j] += v;
+__device__ __forceinline__ void gd_cp8(double* s, const double* g) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(g) : "memory");
+}
+
+__device__ __forceinline__ void gd_stage(double* As, double* Bs, const double* x, int64_t ldx, int nx,
+                                         const double* y, int64_t ldy, int ny, int i0, int j0, int64_t k0,
+                                         int64_t k_end) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int r = 0; r < (GD_T * GD_KC) / 256; ++r) {
+    const int e = tid + 256 * r;
+    const int row = e / GD_KC, kk = e - row * GD_KC;
+    const int64_t k = k0 + kk;
+    double* da = &As[row * GD_LD + kk];
+    double* db = &Bs[row * GD_LD + kk];
+    if (i0 + row < nx && k < k_end)
+      gd_cp8(da, &x[(int64_t)(i0 + row) * ldx + k]);
+    else
+      *da = 0.0;
+    if (j0 + row < ny && k < k_end)
+      gd_cp8(db, &y[(int64_t)(j0 + row) * ldy + k]);
+    else
+      *db = 0.0;
   }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+__global__ void __launch_bounds__(256) k_gram_dmma(int nx, const double* __restrict__ x, int64_t ldx, int ny,
+                                                   const double* __restrict__ y, int64_t ldy, int64_t n,
+                                                   int64_t kchunk, int nsplit, int sym, double* part) {
+  __shared__ __align__(16) double As[2][GD_T * GD_LD];
+  __shared__ __align__(16) double Bs[2][GD_T * GD_LD];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int gq = lane >> 2, tq = lane & 3;
+  const int wi = warp & 1, wj = warp >> 1;
+  const int tiles_i = (nx + GD_T - 1) / GD_T, tiles_j = (ny + GD_T - 1) / GD_T;
+  const int npairs = sym ? tiles_i * (tiles_i + 1) / 2 : tiles_i * tiles_j;
+  const int64_t ntask = (int64_t)npairs * nsplit;
+  for (int64_t task = blockIdx.x; task < ntask; task += gridDim.x) {
+    const int split = (int)(task % nsplit);
+    int tp = (int)(task / nsplit), ti, tj;
+    if (sym) {  // (ti, tj) with ti <= tj, row-major over the upper triangle
+      ti = 0;
+      while (tp >= tiles_i - ti) {
+        tp -= tiles_i - ti;
+        ++ti;
+      }
+      tj = ti + tp;
+    } else {
+      ti = tp / tiles_j;
+      tj = tp - ti * tiles_j;
+    }
+    const int i0 = ti * GD_T, j0 = tj * GD_T;
+    const int64_t k_begin = (int64_t)split * kchunk;
+    const int64_t k_end = min(n, k_begin + kchunk);
+    const int nkc = (int)((k_end - k_begin + GD_KC - 1) / GD_KC);
+    double acc[4][2][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    __syncthreads();  // the buffers of the previous task are consumed
+    if (nkc > 0) gd_stage(As[0], Bs[0], x, ldx, nx, y, ldy, ny, i0, j0, k_begin, k_end);
+    for (int c = 0; c < nkc; ++c) {
+      const int b = c & 1;
+      if (c + 1 < nkc) {
+        gd_stage(As[b ^ 1], Bs[b ^ 1], x, ldx, nx, y, ldy, ny, i0, j0, k_begin + (int64_t)(c + 1) * GD_KC,
+                 k_end);
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+      } else {
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+      }
+      __syncthreads();
+      const double* Ab = As[b] + (wi * 32 + gq) * GD_LD + tq;
+      const double* Bb = Bs[b] + (wj * 16 + gq) * GD_LD + tq;
+#pragma unroll
+      for (int s4 = 0; s4 < GD_KC / 4; ++s4) {
+        double av[4], bv[2];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) av[a] = Ab[a * 8 * GD_LD + 4 * s4];
+#pragma unroll
+        for (int bb = 0; bb < 2; ++bb) bv[bb] = Bb[bb * 8 * GD_LD + 4 * s4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int bb = 0; bb < 2; ++bb) gd_dmma(acc[a][bb], av[a], bv[bb]);
+      }
+      __syncthreads();  // buffer b is free for the chunk after next
+    }
+    double* P = part + (int64_t)split * nx * ny;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int i = i0 + wi * 32 + a * 8 + gq;
+      if (i >= nx) continue;
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb) {
+        const int j = j0 + wj * 16 + bb * 8 + 2 * tq;
+        if (j < ny) P[(int64_t)i * ny + j] = acc[a][bb][0];
+        if (j + 1 < ny) P[(int64_t)i * ny + j + 1] = acc[a][bb][1];
+      }
+    }
+  }
+}
+
+// out[i][j] (+)= sum_split part[split][i][j]; with sym the tiles below the
+// diagonal read the transposed entry of their mirror tile
+__global__ void k_gram_reduce_sym(int nx, int ny, int nsplit, const double* part, double* out, int accumulate,
+                                  int sym) {
+  const int nxy = nx * ny;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nxy; t += gridDim.x * blockDim.x) {
+    const int i = t / ny, j = t - i * ny;
+    const int src = (sym && i / GD_T > j / GD_T) ? j * ny + i : t;
+    double s = 0.0;
+    for (int p = 0; p < nsplit; ++p) s += part[(int64_t)p * nxy + src];
+    out[t] = accumulate ? out[t] + s : s;
+  }
+}
+
+static int gram_dmma_nsplit(int nx, int ny, int64_t n) {
+  const int ti = (nx + GD_T - 1) / GD_T, tj = (ny + GD_T - 1) / GD_T;
+  const int tiles = ti * tj;
+  int64_t want = (148 * 3 + tiles - 1) / tiles;
+  int64_t maxs = (n + 1023) / 1024;
+  if (want > maxs) want = maxs;
+  if (want < 1) want = 1;
+  if (want > 256) want = 256;
+  return (int)want;
+}
+
+size_t gram_dmma_workspace(int nx, int ny, int64_t n) {
+  return (size_t)gram_dmma_nsplit(nx, ny, n) * nx * ny * sizeof(double);
+}
+
+int gram_dmma_run(int nx, const double* x, int64_t ldx, int ny, const double* y, int64_t ldy, int64_t n,
+                  double* out, int accumulate, double* part, cudaStream_t stream) {
+  const int sym = (x == y && ldx == ldy && nx == ny) ? 1 : 0;
+  int nsplit = gram_dmma_nsplit(nx, ny, n);
+  int64_t kchunk = (n + nsplit - 1) / nsplit;
+  kchunk = (kchunk + GD_KC - 1) / GD_KC * GD_KC;
+  nsplit = (int)((n + kchunk - 1) / kchunk);
+  if (nsplit < 1) nsplit = 1;
+  const int ti = (nx + GD_T - 1) / GD_T, tj = (ny + GD_T - 1) / GD_T;
+  const int npairs = sym ? ti * (ti + 1) / 2 : ti * tj;
+  {
+    ProfScope ps("k_gram_dmma", stream);
+    k_gram_dmma<<<grid_for((int64_t)npairs * nsplit, 1, 148 * 4), 256, 0, stream>>>(nx, x, ldx, ny, y, ldy, n,
+                                                                                   kchunk, nsplit, sym, part);
+  }
+  int st = check_launch("gram (tensor cores)");
+  if (st) return st;
+  k_gram_reduce_sym<<<grid_for(nx * ny, 256), 256, 0, stream>>>(nx, ny, nsplit, part, out, accumulate, sym);
+  return check_launch("gram reduce");
+}
+
+// ---------------------------------------------------------------------------
+// T slab: T[pq][j] for determinants J = J0 + j, j < S, pq = p*norb + q
+// ---------------------------------------------------------------------------
+// T slab built 32 determinants per block in shared memory: the alpha
+// and/or beta link contributions of each determinant are added into a
+// zeroed (n^2, 32) tile, which is then written out row by row (coalesced,
+// each T element written once; no separate zeroing pass and no scattered
+// read-modify-write in global memory).  spin: 0 alpha, 1 beta, 2 both.
+constexpr int TT_J = 32, TT_LD = 33;
+
+__global__ void __launch_bounds__(256) k_tslab_tile(int norb, long long Nb, int nla, int nlb,
+                                                    const csffci_link_t* __restrict__ la,
+                                                    const csffci_link_t* __restrict__ lb,
+                                                    const double* __restrict__ c, long long J0, long long S,
+                                                    int spin, double* __restrict__ T) {
+  extern __shared__ double tile[];  // [n^2][TT_LD]
+  const int n2 = norb * norb;
+  const long long nblk = (S + TT_J - 1) / TT_J;
+  for (long long blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+    const long long j0 = blk * TT_J;
+    const int nj = (int)min((long long)TT_J, S - j0);
+    __syncthreads();  // the previous tile is written out
+    for (int i = threadIdx.x; i < n2 * TT_LD; i += blockDim.x) tile[i] = 0.0;
+    __syncthreads();
+    if (spin != 1) {
+      for (int idx = threadIdx.x; idx < nla * TT_J; idx += blockDim.x) {
+        const int l = idx / TT_J, t = idx - l * TT_J;
+        if (t >= nj) continue;
+        const long long J = J0 + j0 + t, ja = J / Nb, jb = J - ja * Nb;
+        const csffci_link_t e = la[ja * nla + l];
+        const int a = e.op & 0xff, i = e.op >> 8;
+        tile[(i * norb + a) * TT_LD + t] += e.sign * c[(long long)e.addr * Nb + jb];
+      }
+      __syncthreads();
+    }
+    if (spin != 0) {
+      for (int idx = threadIdx.x; idx < nlb * TT_J; idx += blockDim.x) {
+        const int l = idx / TT_J, t = idx - l * TT_J;
+        if (t >= nj) continue;
+        const long long J = J0 + j0 + t, ja = J / Nb, jb = J - ja * Nb;
+        const csffci_link_t e = lb[jb * nlb + l];
+        const int a = e.op & 0xff, i = e.op >> 8;
+        tile[(i * norb + a) * TT_LD + t] += e.sign * c[ja * Nb + e.addr];
+      }
+      __syncthreads();
+    }
+    for (int idx = threadIdx.x; idx < n2 * TT_J; idx += blockDim.x) {
+      const int pq = idx / TT_J, t = idx - pq * TT_J;
+      if (t < nj) T[(long long)pq * S + j0 + t] = tile[pq * TT_LD + t];
+    }
+  }
+}
+
+static int tslab_tile_launch(int norb, long long Nb, int nla, int nlb, const csffci_link_t* la,
+                             const csffci_link_t* lb, const double* c, long long J0, long long s, int spin,
+                             double* T, cudaStream_t stream) {
+  const size_t smem = (size_t)norb * norb * TT_LD * sizeof(double);
+  if (smem > 48 * 1024) CSF_CUDA(cudaFuncSetAttribute(k_tslab_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      (int)smem));
+  ProfScope ps("k_tslab_tile", stream);
+  k_tslab_tile<<<grid_for((s + TT_J - 1) / TT_J, 1, 148 * 4), 256, smem, stream>>>(norb, Nb, nla, nlb, la, lb, c,
+                                                                                   J0, s, spin, T);
+  return check_launch("rdm T slab");
 }
 
 __global__ void k_rdm_assemble(int norb, const double* __restrict__ G, const double* __restrict__ d1,
@@ -170,6 +371,20 @@ __global__ void k_rdm_assemble_s(int norb, const double* __restrict__ G, const d
     double v = G[(long long)(q * n + p) * n2 + r * n + s];
     if (d1 && q == r) v -= d1[p * n + s];
     dm2[t] = v;
+  }
+}
+
+// <E_xy> from the Gram of the 2-RDM: sum_r <E_xy E_rr> = <E_xy N> = N <E_xy>
+// (bra and ket both have N electrons of the spin the Gram is taken over),
+// so d1t[x][y] = (1/N) sum_r G[(y,x)][(r,r)] without another pass over T
+__global__ void k_d1_from_gram(int norb, const double* __restrict__ G, double inv_n, double* d1t) {
+  const int n = norb, n2 = n * n;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += gridDim.x * blockDim.x) {
+    const int x = t / n, y = t - x * n;
+    const double* row = G + (long long)(y * n + x) * n2;
+    double acc = 0.0;
+    for (int r = 0; r < n; ++r) acc += row[r * n + r];
+    d1t[t] = acc * inv_n;
   }
 }
 
@@ -208,7 +423,9 @@ size_t csffci_rdm12_workspace(int norb, int neleca, int nelecb) {
   size_t t = (size_t)(2 * S * n2) * sizeof(double);
   size_t g = (size_t)(n2 * n2 + 2 * n2) * sizeof(double);
   size_t part = gram_workspace((int)n2, (int)n2, S);
+  size_t partd = gram_dmma_workspace((int)n2, (int)n2, S);
   size_t part1 = gram_workspace(1, (int)n2, S);
+  if (partd > part) part = partd;
   return t + g + (part > part1 ? part : part1) + 1024;
 }
 
@@ -239,25 +456,20 @@ int csffci_rdm12(int norb, int neleca, int nelecb, const csffci_link_t* link_a,
     for (int which = 0; which < (same ? 1 : 2); ++which) {
       double* T = which == 0 ? Tk : Tb;
       const double* c = which == 0 ? ket : bra;
-      k_zero<<<grid_for(s * n2, 256, 148 * 16), 256, 0, stream>>>(T, s * n2);
-      if ((st = check_launch("rdm T zero"))) return st;
-      if (nla > 0) {
-        k_tslab_links<<<grid_for(s * nla, 256, 148 * 16), 256, 0, stream>>>(
-            norb, Nb, nla, nlb, link_a, link_b, c, J0, s, 0, T);
-        if ((st = check_launch("rdm T alpha"))) return st;
-      }
-      if (nlb > 0) {
-        k_tslab_links<<<grid_for(s * nlb, 256, 148 * 16), 256, 0, stream>>>(
-            norb, Nb, nla, nlb, link_a, link_b, c, J0, s, 1, T);
-        if ((st = check_launch("rdm T beta"))) return st;
-      }
+      if ((st = tslab_tile_launch(norb, Nb, nla, nlb, link_a, link_b, c, J0, s, 2, T, stream))) return st;
     }
     const double* TB = same ? Tk : Tb;
-    // d1t[qp] = sum_J bra_J Tk[qp][J]  -> dm1[p][q] after the transpose
-    if ((st = gram_run(1, bra + J0, s, n2, Tk, s, s, d1t, accumulate, part, stream))) return st;
     if (dm2) {
-      if ((st = gram_run(n2, TB, s, n2, Tk, s, s, G, accumulate, part, stream))) return st;
+      if ((st = gram_dmma_run(n2, TB, s, n2, Tk, s, s, G, accumulate, part, stream))) return st;
+    } else {
+      // d1t[qp] = sum_J bra_J Tk[qp][J]  -> dm1[p][q] after the transpose
+      if ((st = gram_run(1, bra + J0, s, n2, Tk, s, s, d1t, accumulate, part, stream))) return st;
     }
+  }
+  if (dm2) {
+    const int ne = neleca + nelecb;
+    k_d1_from_gram<<<grid_for(n2, 256), 256, 0, stream>>>(norb, G, ne > 0 ? 1.0 / ne : 0.0, d1t);
+    if ((st = check_launch("rdm1 from the Gram"))) return st;
   }
   k_transpose_small<<<grid_for(n2, 256), 256, 0, stream>>>(norb, d1t, dm1);
   if ((st = check_launch("rdm1 transpose"))) return st;
@@ -280,7 +492,9 @@ size_t csffci_rdm12s_workspace(int norb, int neleca, int nelecb) {
   size_t t = (size_t)(4 * S * n2) * sizeof(double);
   size_t g = (size_t)(3 * n2 * n2 + 4 * n2) * sizeof(double);
   size_t part = gram_workspace((int)n2, (int)n2, S);
+  size_t partd = gram_dmma_workspace((int)n2, (int)n2, S);
   size_t part1 = gram_workspace(1, (int)n2, S);
+  if (partd > part) part = partd;
   return t + g + (part > part1 ? part : part1) + 1024;
 }
 
@@ -322,30 +536,26 @@ int csffci_rdm12s(int norb, int neleca, int nelecb, const csffci_link_t* link_a,
       const double* c = which == 0 ? ket : bra;
       double* Ta = which == 0 ? Tka : Tba;
       double* Tb = which == 0 ? Tkb : Tbb;
-      k_zero<<<grid_for(s * n2, 256, 148 * 16), 256, 0, stream>>>(Ta, s * n2);
-      if ((st = check_launch("rdm12s T zero"))) return st;
-      k_zero<<<grid_for(s * n2, 256, 148 * 16), 256, 0, stream>>>(Tb, s * n2);
-      if ((st = check_launch("rdm12s T zero"))) return st;
-      if (nla > 0) {
-        k_tslab_links<<<grid_for(s * nla, 256, 148 * 16), 256, 0, stream>>>(
-            norb, Nb, nla, nlb, link_a, link_b, c, J0, s, 0, Ta);
-        if ((st = check_launch("rdm12s T alpha"))) return st;
-      }
-      if (nlb > 0) {
-        k_tslab_links<<<grid_for(s * nlb, 256, 148 * 16), 256, 0, stream>>>(
-            norb, Nb, nla, nlb, link_a, link_b, c, J0, s, 1, Tb);
-        if ((st = check_launch("rdm12s T beta"))) return st;
-      }
+      if ((st = tslab_tile_launch(norb, Nb, nla, nlb, link_a, link_b, c, J0, s, 0, Ta, stream))) return st;
+      if ((st = tslab_tile_launch(norb, Nb, nla, nlb, link_a, link_b, c, J0, s, 1, Tb, stream))) return st;
     }
     const double* BA = same ? Tka : Tba;
     const double* BB = same ? Tkb : Tbb;
-    if ((st = gram_run(1, bra + J0, s, n2, Tka, s, s, d1at, accumulate, part, stream))) return st;
-    if ((st = gram_run(1, bra + J0, s, n2, Tkb, s, s, d1bt, accumulate, part, stream))) return st;
     if (two) {
-      if ((st = gram_run(n2, BA, s, n2, Tka, s, s, Gaa, accumulate, part, stream))) return st;
-      if ((st = gram_run(n2, BA, s, n2, Tkb, s, s, Gab, accumulate, part, stream))) return st;
-      if ((st = gram_run(n2, BB, s, n2, Tkb, s, s, Gbb, accumulate, part, stream))) return st;
+      if ((st = gram_dmma_run(n2, BA, s, n2, Tka, s, s, Gaa, accumulate, part, stream))) return st;
+      if ((st = gram_dmma_run(n2, BA, s, n2, Tkb, s, s, Gab, accumulate, part, stream))) return st;
+      if ((st = gram_dmma_run(n2, BB, s, n2, Tkb, s, s, Gbb, accumulate, part, stream))) return st;
+    } else {
+      if ((st = gram_run(1, bra + J0, s, n2, Tka, s, s, d1at, accumulate, part, stream))) return st;
+      if ((st = gram_run(1, bra + J0, s, n2, Tkb, s, s, d1bt, accumulate, part, stream))) return st;
     }
+  }
+  if (two) {
+    // same-spin Grams: sum_r <E^s_xy E^s_rr> = N_s <E^s_xy>
+    k_d1_from_gram<<<grid_for(n2, 256), 256, 0, stream>>>(norb, Gaa, neleca > 0 ? 1.0 / neleca : 0.0, d1at);
+    if ((st = check_launch("rdm1a from the Gram"))) return st;
+    k_d1_from_gram<<<grid_for(n2, 256), 256, 0, stream>>>(norb, Gbb, nelecb > 0 ? 1.0 / nelecb : 0.0, d1bt);
+    if ((st = check_launch("rdm1b from the Gram"))) return st;
   }
   k_transpose_small<<<grid_for(n2, 256), 256, 0, stream>>>(norb, d1at, dm1a);
   if ((st = check_launch("rdm1a transpose"))) return st;
