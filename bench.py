@@ -16,6 +16,9 @@ region).  ``roofline`` reports the sigma kernel against HBM with the
 algorithmic bytes 8*ndet*2*(nlink_a+nlink_b) per launch.  N>1: independent
 replicas, one per GPU (the path does not shard); value is the sum.
 
+``rdm`` (same line, rank 0 at N=1): device time of the adjoint (RDM) kernel
+at CAS(16,16) (one root) and CAS(14,14) (two roots state-averaged).
+
 ``batched`` (same line, rank 0 at N=1): solves+RDMs/s of 128 seeded uneven
 problems through the device-resident batched solver, next to the plain
 one-problem-at-a-time GPU form on the same problems (run_batched).
@@ -318,10 +321,53 @@ def run_ours(args, rank_env):
         v, cores, sample = cpu_reference_sigma(NORB, NELEC, RANK, budget_s=20.0)
         line["cpu_baseline"] = {"value": v, "unit": "sigma/s", "cores": cores, "kind": "reference",
                                 "sample": sample}
+    if rank == 0 and world == 1 and not args.no_rdm:
+        line["rdm"] = run_rdm(dmma)
     if rank == 0 and world == 1 and not args.no_batched:
         line["batched"] = run_batched(args.batch)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def run_rdm(dmma_peak, cases=None):
+    """The adjoint (RDM) kernel on the sizes of the large configurations,
+    device-timed: the CAS(16,16) singlet 2-RDM of one root, and the
+    state-averaged 1-/2-RDMs of two CAS(14,14) (7,7) roots (the backward of
+    the differentiable state-averaged energy).  Vectors are random unit
+    vectors of those spaces (the kernel's cost does not depend on them)."""
+    import torch
+    from math import comb
+    from pyscf_forge_b200.fci import direct_spin1 as D
+    out = {}
+    for tag, norb, nelec, nroots in (("cas16_singlet_1root", 16, (8, 8), 1), ("cas14_sa2", 14, (7, 7), 2)):
+        if cases and tag not in cases:
+            continue
+        n = comb(norb, nelec[0]) * comb(norb, nelec[1])
+        g = torch.Generator(device="cuda").manual_seed(3)
+        cs = [torch.randn(n, dtype=torch.float64, device="cuda", generator=g) for _ in range(nroots)]
+        cs = [c / torch.linalg.norm(c) for c in cs]
+        D.dev_rdm12(cs[0], None, norb, nelec)  # warm-up (workspace)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dm1 = dm2 = None
+        for c in cs:
+            d1, d2 = D.dev_rdm12(c, None, norb, nelec)
+            dm1 = d1 / nroots if dm1 is None else dm1 + d1 / nroots
+            dm2 = d2 / nroots if dm2 is None else dm2 + d2 / nroots
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        flops = nroots * 2.0 * n * norb ** 4
+        out[tag] = {"ms": ms, "determinants": n, "roots": nroots,
+                    "gram_tflops": flops / (ms * 1e-3) / 1e12,
+                    "frac_dmma": flops / (ms * 1e-3) / 1e12 / dmma_peak,
+                    "trace_dm1": float(torch.trace(dm1))}
+    out["note"] = ("adjoint = transition-density / RDM kernel: T slabs <J|E_pq|c> built in shared memory, "
+                   "Gram on FP64 DMMA (bra == ket: symmetric half), 1-RDM from the Gram; flops counted "
+                   "as the dense 2*ndet*norb^4")
+    return out
 
 
 def run_batched(nprob):
@@ -375,12 +421,23 @@ def main():
                     help="cas16 is the benchmark; the smaller ones exist for profiling captures")
     ap.add_argument("--no-e2e", action="store_true", help="time the device loop only (profiling)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-solves measurement")
+    ap.add_argument("--no-rdm", action="store_true", help="skip the RDM (adjoint) timing")
+    ap.add_argument("--rdm-only", default="", help="only the RDM timing of these cases "
+                    "(cas16_singlet_1root,cas14_sa2), for profiling captures")
     ap.add_argument("--batch", type=int, default=128, help="problems in the batched-solves measurement")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
         run_reference(args, (rank, world))
+        return
+    if args.rdm_only:
+        # the adjoint timing alone (profiling captures of the RDM kernels)
+        import torch
+        from pyscf_forge_b200 import _capi
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        if rank == 0:
+            print(json.dumps(run_rdm(_capi.fp64_peak(0), args.rdm_only.split(","))), flush=True)
         return
     if world > 1:
         import datetime
