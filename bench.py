@@ -62,6 +62,17 @@ def seeded_integrals(norb, rank, seed=0):
     return h1, eri
 
 
+def max_over_ranks(x, world, device="cuda"):
+    """The largest of a per-rank time over all ranks (every rank returns it):
+    multi-GPU numbers are reported for the slowest replica."""
+    if world <= 1:
+        return float(x)
+    import torch
+    tt = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+    return float(tt.item())
+
+
 def algorithmic(norb, nelec):
     from math import comb
     na, nb = nelec
@@ -259,10 +270,7 @@ def run_ours(args, rank_env):
     prof = _capi.profile_report()
     _capi.profile_enable(False)
     ms = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        tt = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(ms, world)
     value = world * 1000.0 / ms
     k_cnt, k_ms = prof.get("k_sigma_rr", prof.get("k_sigma", (0, 0.0)))
     k_avg_ms = k_ms / max(k_cnt, 1)
@@ -282,10 +290,7 @@ def run_ours(args, rank_env):
         res = sol.contract_2e(h2eff, ch, NORB, NELEC)
     barrier()
     e2e_ms = (time.perf_counter() - t0) * 1000.0 / e2e_steps
-    if world > 1:
-        tt = torch.tensor([e2e_ms], device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+    e2e_ms = max_over_ranks(e2e_ms, world)
     # the public-API result must equal the device step
     step()
     torch.cuda.synchronize()

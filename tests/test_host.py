@@ -83,3 +83,36 @@ def test_state_weights_validation():
     for bad in ([], [[0.5, 0.5]], [0.5, float("nan")], [1.5, -0.5], [0.5, 0.4]):
         with pytest.raises(ValueError):
             validate_state_weights(bad)
+
+
+def _max_rank_worker(rank, world, port, q):
+    import os
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import bench
+        q.put((rank, bench.max_over_ranks(1.5 + rank, world, device="cpu")))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_bench_max_over_ranks_gloo():
+    """The multi-replica timing reduction of bench.py (max over ranks) on
+    two gloo ranks: every rank sees the slowest rank's time."""
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_max_rank_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    assert all(p.exitcode == 0 for p in procs)
+    got = dict(q.get(timeout=5) for _ in range(2))
+    assert got == {0: 2.5, 1: 2.5}
