@@ -41,7 +41,10 @@ enum {
 
 /* One spin-string excitation a+_cre a_des |I> = sign |addr>; byte layout of
  * gas_link_entry_t in raw format (pyscf/lib/mcscf/fci_gas.h:94-105):
- * op = cre | des << 8. */
+ * op = cre | des << 8.  pad (the padding byte there) holds the pair index
+ * hi*(hi+1)/2+lo of (cre, des), written by csffci_link_table for norb <= 22;
+ * the sigma kernels read it, so the tables they are given come from
+ * csffci_link_table, 8-byte aligned. */
 typedef struct {
   uint32_t addr;
   uint16_t op;
@@ -85,9 +88,10 @@ const char* csffci_last_error(void);
 int csffci_profile_enable(int on);
 int csffci_profile_report(char* buf, size_t len);
 /* FP64 throughput of a register-only loop on the current device (kind 0:
- * DMMA m8n8k4, kind 1: DFMA), in TFLOP/s; synchronises the stream.  The
- * FP64 roofline denominator for the sigma kernel.  No counterpart in the
- * reference. */
+ * DMMA m8n8k4 at 16 warps per SM, kind 1: DFMA, kind 2: DMMA at 17 warps per
+ * SM, one CTA of 544 threads, which loads one of the four schedulers with 5
+ * warps), in TFLOP/s; synchronises the stream.  Kind 0 is the FP64 roofline
+ * denominator for the sigma kernel.  No counterpart in the reference. */
 int csffci_fp64_peak(int kind, int iters, double* tflops, cudaStream_t stream);
 
 /* ---- strings and link tables (PySCF cistring; reference twin

@@ -91,7 +91,7 @@ int csffci_profile_enable(int on) {
 }
 
 int csffci_fp64_peak(int kind, int iters, double* tflops, cudaStream_t stream) {
-  CSF_REQUIRE(tflops != nullptr && iters > 0 && (kind == 0 || kind == 1), "fp64_peak: bad arguments");
+  CSF_REQUIRE(tflops != nullptr && iters > 0 && kind >= 0 && kind <= 2, "fp64_peak: bad arguments");
   int dev = 0, nsm = 148;
   CSF_CUDA(cudaGetDevice(&dev));
   CSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -100,11 +100,12 @@ int csffci_fp64_peak(int kind, int iters, double* tflops, cudaStream_t stream) {
   cudaEvent_t a, b;
   CSF_CUDA(cudaEventCreate(&a));
   CSF_CUDA(cudaEventCreate(&b));
-  const int blocks = nsm * 2, threads = 256;
-  if (kind == 0) k_peak_dmma<<<blocks, threads, 0, stream>>>(sink, 64);
+  // kind 2: one CTA of 17 warps per SM (a scheduler with 5 warps)
+  const int blocks = kind == 2 ? nsm : nsm * 2, threads = kind == 2 ? 544 : 256;
+  if (kind != 1) k_peak_dmma<<<blocks, threads, 0, stream>>>(sink, 64);
   else k_peak_dfma<<<blocks, threads, 0, stream>>>(sink, 64);
   cudaEventRecord(a, stream);
-  if (kind == 0) k_peak_dmma<<<blocks, threads, 0, stream>>>(sink, iters);
+  if (kind != 1) k_peak_dmma<<<blocks, threads, 0, stream>>>(sink, iters);
   else k_peak_dfma<<<blocks, threads, 0, stream>>>(sink, iters);
   cudaEventRecord(b, stream);
   CSF_CUDA(cudaEventSynchronize(b));
@@ -113,7 +114,7 @@ int csffci_fp64_peak(int kind, int iters, double* tflops, cudaStream_t stream) {
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   const double warps = (double)blocks * threads / 32.0;
-  const double flops = kind == 0 ? 2.0 * 8 * 8 * 4 * 8 * (double)iters * warps
+  const double flops = kind != 1 ? 2.0 * 8 * 8 * 4 * 8 * (double)iters * warps
                                  : 2.0 * 8 * (double)iters * blocks * threads;
   *tflops = flops / (ms * 1e-3) / 1e12;
   return check_launch("fp64_peak");

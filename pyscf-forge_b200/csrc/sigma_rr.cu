@@ -36,13 +36,16 @@ namespace csffci {
 
 bool sigma_rr_supported(int norb) { return norb >= 4 && norb <= 16; }
 
+// the tile loops read link entries as 8-byte words and copy 8-byte elements
+static bool rr_aligned8(const void* p) { return ((uintptr_t)p & 7u) == 0; }
+
 // Tile shapes (rows per warp, n-tiles of 8 columns): 16-row warps halve
 // the B-fragment traffic but need 2*KS + 4*NT doubles of registers per lane;
 // with 9 warps (norb 15,16) an SMSP holds 3 warps, i.e. at most 168
 // registers, so those sizes have no (16, 4) instance.  The defaults are the
 // fastest shapes measured on B200 for one singlet/doublet problem: (16, 2)
-// up to norb 10, (8, 2) for 11-12, (8, 4) from 13 (the two-n-tile shapes
-// run 2-3 CTAs per SM at small norb); CSFFCI_SIGMA_VARIANT overrides them
+// up to norb 10 and at 13, (8, 2) for 11-12, (8, 4) from 14 (the two-n-tile
+// shapes run 2-3 CTAs per SM at small norb); CSFFCI_SIGMA_VARIANT overrides them
 // and the batched solver's autotuner picks per orbital count.
 static const int kVariantShape[RR_NVARIANT][2] = {{16, 4}, {8, 4}, {16, 2}, {8, 2}};
 
@@ -54,7 +57,7 @@ int rr_default_variant(int norb) {
     const int v = atoi(env);
     if (rr_variant_valid(norb, v)) return v;
   }
-  return norb <= 10 ? 2 : norb <= 12 ? 3 : 1;
+  return norb <= 10 || norb == 13 ? 2 : norb <= 12 ? 3 : 1;
 }
 
 // fill the bookkeeping fields of the jobs; returns the largest Nb, nla, nlb
@@ -115,9 +118,10 @@ int sigma_rr_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev,
   g.off_d = take((size_t)2 * g.nd_rows * g.ds * sizeof(double));
   g.off_l = take((size_t)2 * nb * g.ls * sizeof(csffci_link_t));
   g.off_crow = take((size_t)max_nb * sizeof(double));
-  g.off_las = take((size_t)(max_nla > 0 ? max_nla : 1) * sizeof(csffci_link_t));
-  g.off_rowsrc = take((size_t)g.nd_rows * sizeof(int));
-  g.off_zrow = take((size_t)(npair + 2) * sizeof(int));
+  g.off_al = take((size_t)(max_nla > 0 ? max_nla : 1) * sizeof(RRAlpha));
+  g.off_zl = take((size_t)npair * sizeof(int));
+  g.off_pn = take((size_t)2 * npair * sizeof(unsigned));
+  g.off_zf = take((size_t)npair * sizeof(int));
   const size_t smem = off;
   if (smem > 227 * 1024 - 256) {
     set_error("sigma: tile of %zu bytes exceeds shared memory", smem);
@@ -134,6 +138,8 @@ switch (variant) {
 int sigma_rr_run(int norb, int neleca, int nelecb, const double* h2e, const csffci_link_t* la,
                  const csffci_link_t* lb, const double* ci, double* out, bool sym, double eta,
                  cudaStream_t stream) {
+  CSF_REQUIRE(rr_aligned8(la) && rr_aligned8(lb) && rr_aligned8(ci) && rr_aligned8(out),
+              "sigma: link tables and vectors must be 8-byte aligned");
   csffci_sigma_job_t J;
   memset(&J, 0, sizeof(J));
   J.h2e = h2e;
@@ -208,6 +214,9 @@ int sigma_batch_prepare(int norb, int njobs, csffci_sigma_job_t* jobs, SigmaBatc
     CSF_REQUIRE(!J.sym || (J.neleca == J.nelecb && J.scratch != nullptr && (J.eta == 1 || J.eta == -1)),
                 "sigma_batch: job %d: spin-symmetric mode needs neleca == nelecb, eta = +-1 and scratch", i);
     CSF_REQUIRE(J.h2e && J.link_a && J.link_b && J.ci && J.sigma, "sigma_batch: job %d has a NULL pointer", i);
+    CSF_REQUIRE(rr_aligned8(J.link_a) && rr_aligned8(J.link_b) && rr_aligned8(J.ci) && rr_aligned8(J.sigma) &&
+                    rr_aligned8(J.scratch),
+                "sigma_batch: job %d has a pointer that is not 8-byte aligned", i);
   }
   info->norb = norb;
   info->njobs = njobs;

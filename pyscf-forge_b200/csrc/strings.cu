@@ -41,6 +41,15 @@ __global__ void k_gen_strings(int norb, int nelec, unsigned long long n, uint64_
     out[i] = str_unrank(norb, nelec, i);
 }
 
+// Byte 7 of an entry: the pair index hi*(hi+1)/2+lo of (p, q), the row of
+// the four-fold h2e that the sigma tile loops address directly (it fits a
+// byte up to 22 orbitals; 0 above).
+__device__ __forceinline__ uint8_t link_pair_byte(int p, int q) {
+  const int hi = p > q ? p : q, lo = p > q ? q : p;
+  const int pr = hi * (hi + 1) / 2 + lo;
+  return (uint8_t)(pr < 256 ? pr : 0);
+}
+
 // One thread per source string; entries in the order of
 // pyscf/lib/mcscf/fci_string_gas.c:1341-1382: for each occupied q
 // ascending, (q,q) first, then each virtual p ascending.  Sign of
@@ -62,7 +71,7 @@ __global__ void k_link_table(int norb, int nelec, unsigned long long nstr, int n
       e.addr = (uint32_t)ia;
       e.op = (uint16_t)(q | (q << 8));
       e.sign = 1;
-      e.pad = 0;
+      e.pad = link_pair_byte(q, q);
       row[k++] = e;
       unsigned long long vir = (~s) & full;
       while (vir) {
@@ -74,6 +83,7 @@ __global__ void k_link_table(int norb, int nelec, unsigned long long nstr, int n
         e.addr = (uint32_t)str_rank(s1);
         e.op = (uint16_t)(p | (q << 8));
         e.sign = (int8_t)(1 - 2 * (__popcll(s & mask) & 1));
+        e.pad = link_pair_byte(p, q);
         row[k++] = e;
       }
     }
