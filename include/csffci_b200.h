@@ -113,6 +113,19 @@ int csffci_csd_masks(int norb, int neleca, int nelecb, int smult,
                      uint32_t* csd_mask, uint32_t* econf_det_mask,
                      uint32_t* econf_csf_mask, cudaStream_t stream);
 
+/* conf_ok[c] = 1 for the configurations c whose total occupation per GAS
+ * subspace (alpha + beta electrons in the gas_norb[g] consecutive orbitals of
+ * subspace g) is one of the nsupergroup rows of supergroups (int32
+ * [nsupergroup][ngas], host memory); 0 otherwise.  econf_det_mask (device,
+ * from csffci_csd_masks) maps determinants to configurations; conf_ok is a
+ * device array over the configurations.  This is the configuration form of
+ * a spin-complete GAS restriction (the reference's spin-supergroup set D,
+ * pyscf/mcscf/addons_gas.py:318-428, 782-798).  ngas <= 10, nsupergroup
+ * <= 1024. */
+int csffci_gas_conf_mask(int norb, int neleca, int nelecb, const uint32_t* econf_det_mask, int ngas,
+                         const int32_t* gas_norb, int nsupergroup, const int32_t* supergroups,
+                         uint8_t* conf_ok, cudaStream_t stream);
+
 /* ---- genealogical spin couplings (csfstring.py:806-960, csfstring.c:86-293) */
 
 /* umat[det][csf] for nspin unpaired electrons, 2MS = neleca-nelecb, 2S+1 =

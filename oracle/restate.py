@@ -263,6 +263,46 @@ def make_confsym(norb, neleca, nelecb, econf_det_mask, orbsym):
     return ia[addr // nb] ^ ib[addr % nb]
 
 
+def gas_allowed_dets(norb, neleca, nelecb, gas_orbs, blocks):
+    """Determinants of a GAS space in full-CAS (alpha-major, colex) order:
+    those whose (alpha occupation of each subspace, beta occupation of each
+    subspace) is a row of the spin-supergroup set D -- the membership rule of
+    the reference's GAS space, gas_space_from_blocks
+    (pyscf/lib/mcscf/fci_string_gas.c:1683-1704) over the blocks of
+    pyscf/mcscf/addons_gas.py:318-428, with subspace g the next gas_orbs[g]
+    orbitals."""
+    ngas = len(gas_orbs)
+    starts = np.concatenate([[0], np.cumsum(gas_orbs)[:-1]]).astype(np.int64)
+    masks = [((1 << int(n)) - 1) << int(st) for n, st in zip(gas_orbs, starts)]
+    rows = {tuple(int(v) for v in r) for r in np.asarray(blocks)}
+
+    def occ(strs):
+        return np.array([[_popcount(int(st) & m) for m in masks] for st in strs], dtype=np.int64)
+
+    oa = occ(gen_strings(norb, neleca))
+    ob = occ(gen_strings(norb, nelecb))
+    out = np.zeros((oa.shape[0], ob.shape[0]), dtype=bool)
+    for i in range(oa.shape[0]):
+        for j in range(ob.shape[0]):
+            out[i, j] = tuple(oa[i].tolist() + ob[j].tolist()) in rows
+    assert len(next(iter(rows))) == 2 * ngas
+    return out
+
+
+def make_confgas(econf_det_mask, allowed_dets):
+    """Per configuration, whether its determinants are in the GAS space (for
+    a spin-complete set all determinants of a configuration agree)."""
+    econf = np.asarray(econf_det_mask, dtype=np.int64).ravel()
+    allowed = np.asarray(allowed_dets, dtype=bool).ravel()
+    nconf = int(econf.max()) + 1
+    hit = np.zeros(nconf, dtype=np.int64)
+    tot = np.zeros(nconf, dtype=np.int64)
+    np.add.at(hit, econf, allowed.astype(np.int64))
+    np.add.at(tot, econf, 1)
+    assert np.all((hit == 0) | (hit == tot)), "GAS set is not a union of configurations"
+    return hit > 0
+
+
 def gen_addrs2str(nspin, smult, addrs):
     """csfstring.c:243-293 (coupling string of a genealogical address)."""
     g = csf_gentable(nspin, smult)

@@ -60,3 +60,9 @@ def gen_des_str_index(orb_list, nelec):
                 out[k, j] = (0, p, tgt[s ^ (1 << p)], _sign_above(p, s))
                 j += 1
     return out
+
+
+def make_strings(orb_list, nelec):
+    """Occupation strings of nelec electrons in orb_list (role of
+    cistring.make_strings)."""
+    return gen_strings4orblist(orb_list, nelec)

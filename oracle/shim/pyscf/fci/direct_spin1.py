@@ -56,6 +56,8 @@ def make_pspace_precond(hdiag, pspaceig, pspaceci, addr, level_shift=0):
 
 
 class FCISolver(lib.StreamObject):
+    _keys = {"max_memory", "nroots", "davidson_only", "conv_tol", "conv_tol_residual", "lindep",
+             "max_cycle", "max_space", "level_shift", "pspace_size", "spin", "verbose", "mol"}
     max_memory = 64000
     nroots = 1
     davidson_only = False
@@ -104,3 +106,18 @@ class FCISolver(lib.StreamObject):
 
     def make_rdm12(self, civec, norb, nelec, link_index=None, reorder=True):
         return gasref.make_rdm12(civec, civec, norb, _unpack_nelec(nelec))
+
+
+def _not_in_stand_in(name):
+    def fn(*a, **k):
+        raise NotImplementedError("direct_spin1.%s is not part of the stand-in" % name)
+    fn.__name__ = name
+    fn.__doc__ = "direct_spin1.%s (not part of the stand-in)" % name
+    return fn
+
+
+# names the reference's GAS solver (pyscf/mcscf/fci_gas.py) refers to; its
+# GAS kernels replace them, so the stand-in only has to provide the names
+for _n in ("make_rdm1", "make_rdm1s", "make_rdm12", "make_rdm12s",
+           "trans_rdm1", "trans_rdm1s", "trans_rdm12", "trans_rdm12s"):
+    globals()[_n] = _not_in_stand_in(_n)

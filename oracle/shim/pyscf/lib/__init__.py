@@ -36,6 +36,8 @@ class _FakeLibfci:
 def load_library(name):
     if name == "libcsf":
         return gasref.lib_csf()
+    if name == "libfci_gas":
+        return ctypes.CDLL(os.path.join(gasref.REF_DIR, "libfci_gas.so"))
     if name == "libfci":
         return _FakeLibfci()
     raise OSError(name)
@@ -73,3 +75,16 @@ def takebak_2d(out, a, idx, idy):
     """out[idx[:, None], idy] += a (role of lib.takebak_2d)."""
     out[np.ix_(np.asarray(idx), np.asarray(idy))] += a
     return out
+
+
+def isinteger(obj):
+    """Integer scalars (Python or numpy), not bool (role of lib.isinteger)."""
+    return isinstance(obj, (int, np.integer)) and not isinstance(obj, (bool, np.bool_))
+
+
+def with_doc(doc):
+    """Decorator setting __doc__ (role of lib.with_doc)."""
+    def deco(fn):
+        fn.__doc__ = doc
+        return fn
+    return deco

@@ -128,6 +128,7 @@ _SIGS = {
     "csffci_fp64_peak": ([_i, _i, ctypes.POINTER(_d), _p], _i),
     "csffci_gen_strings": ([_i, _i, _p, _p], _i),
     "csffci_link_table": ([_i, _i, _p, _p], _i),
+    "csffci_gas_conf_mask": ([_i, _i, _i, _p, _i, _p, _i, _p, _p, _p], _i),
     "csffci_csd_masks": ([_i, _i, _i, _i, _p, _p, _p, _p], _i),
     "csffci_spin_evecs": ([_i, _i, _i, _i, _p, _p], _i),
     "csffci_spin_exchange_table": ([_i, _i, _i, _i, _p, _p, _p], _i),

@@ -19,6 +19,7 @@ from .._runtime import device, eri_pair_matrix, like_input, ptr, require_cuda, s
 from ..fci import direct_spin1
 from ..fci.davidson import DiagPrecond, davidson, gram
 from ..fci.direct_spin1 import _unpack_nelec
+from . import gas as _gas
 from .csfstring import CSFTransformer, count_all_csfs
 
 
@@ -391,14 +392,35 @@ class FCIBase:
 
 
 class CSFFCISolver:
-    """csf.py:499-555."""
-    _keys = {'smult', 'transformer'}
+    """csf.py:499-555.  With gas_orbs set, the CSF space is restricted to the
+    configurations a GAS restriction allows (gas_orbs, gas_restr and
+    gas_restr_type as the reference's GAS solver takes them,
+    pyscf/mcscf/fci_gas.py:778-801; the restriction has to be spin
+    complete, see csf_fci.gas)."""
+    _keys = {'smult', 'transformer', 'gas_orbs', 'gas_restr', 'gas_restr_type'}
     pspace_size = 200
+    gas_orbs = None
+    gas_restr = None
+    gas_restr_type = _gas.GAS_RESTR_SPIN_SUPERGROUP
 
     def __init__(self, mol=None, smult=None):
         self.smult = smult
         self.transformer = None
         super().__init__(mol)
+
+    def gas_spec(self, norb=None, nelec=None):
+        """(subspace sizes, spin-free supergroups) of the GAS restriction for
+        (norb, nelec), or None without one."""
+        if self.gas_orbs is None:
+            return None
+        norb = self.norb if norb is None else norb
+        nelec = _unpack_nelec(self.nelec if nelec is None else nelec)
+        if sum(int(n) for n in self.gas_orbs) != int(norb):
+            raise ValueError("sum(gas_orbs) must equal norb")
+        return _gas.spin_free_supergroups(self.gas_orbs, nelec, self.gas_restr, self.gas_restr_type)
+
+    def _apply_gas(self):
+        self.transformer.gas = self.gas_spec()
 
     def make_hdiag(self, h1e, eri, norb, nelec, compress=False):
         out = make_hdiag_det(self, h1e, eri, norb, nelec)
@@ -492,4 +514,6 @@ class FCISolver(CSFFCISolver, FCIBase):
             self.transformer = CSFTransformer(self.norb, neleca, nelecb, self.smult,
                                               max_memory=self.max_memory)
         else:
+            self.transformer.gas = None
             self.transformer._update_spin_cache(self.norb, neleca, nelecb, self.smult)
+        self._apply_gas()

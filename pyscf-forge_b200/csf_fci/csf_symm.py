@@ -142,6 +142,8 @@ class FCISolver(_csf.FCISolver):
             self.transformer = CSFTransformer(self.norb, neleca, nelecb, self.smult, orbsym=self.orbsym,
                                               wfnsym=wfnsym, max_memory=self.max_memory)
         else:
+            self.transformer.gas = None
             self.transformer._update_spin_cache(self.norb, neleca, nelecb, self.smult)
             self.transformer._update_symm_cache(self.orbsym)
             self.transformer.wfnsym = wfnsym
+        self._apply_gas()

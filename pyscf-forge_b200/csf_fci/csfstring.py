@@ -165,16 +165,19 @@ def _block_sign(npair, nelecb):
 class CSFTransformer:
     """GPU counterpart of csfstring.CSFTransformer (csfstring.py:33-223)."""
 
-    def __init__(self, norb, neleca, nelecb, smult, orbsym=None, wfnsym=None, max_memory=None):
+    def __init__(self, norb, neleca, nelecb, smult, orbsym=None, wfnsym=None, max_memory=None, gas=None):
         require_cuda()
         self._norb = self._neleca = self._nelecb = self._smult = None
         self._orbsym = None
         self.confsym = None
+        self._gas = None
+        self.confgas = None
         self._symcache = {}
         self.wfnsym = wfnsym
         self.max_memory = max_memory
         self._update_spin_cache(norb, neleca, nelecb, smult)
         self.orbsym = orbsym
+        self.gas = gas
 
     # ---- cache -----------------------------------------------------------
     def _update_spin_cache(self, norb, neleca, nelecb, smult):
@@ -208,6 +211,9 @@ class CSFTransformer:
         self._symcache = {}
         if self._orbsym is not None:
             self.confsym = make_confsym(norb, neleca, nelecb, self.econf_det_mask, self._orbsym)
+        self.confgas = None
+        if self._gas is not None:
+            self.confgas = make_confgas(norb, neleca, nelecb, self.econf_det_mask, self._gas)
 
     def _update_symm_cache(self, orbsym):
         """csfstring.py:117-120: configuration irreps for a new orbsym."""
@@ -223,32 +229,76 @@ class CSFTransformer:
             self.confsym = None
         self._orbsym = orbsym
 
-    def _sym(self):
-        """Packing of the CSF vector to the CSFs whose configuration has the
-        irrep wfnsym (csfstring.py:74-88): per block the selected
-        configurations and their packed offsets.  None without symmetry."""
-        if self.wfnsym is None or self._orbsym is None:
+    # ---- GAS restriction ---------------------------------------------------
+    @property
+    def gas(self):
+        """(subspace sizes, spin-free supergroup rows) of a GAS restriction,
+        or None (csf_fci.gas.spin_free_supergroups gives this form)."""
+        return self._gas
+
+    @gas.setter
+    def gas(self, spec):
+        if spec is not None:
+            orbs, sg = spec
+            orbs = tuple(int(n) for n in orbs)
+            sg = np.ascontiguousarray(np.asarray(sg, dtype=np.int32).reshape(-1, len(orbs)))
+            if sum(orbs) != self._norb:
+                raise ValueError("GAS subspaces hold %d orbitals, the space has %d" % (sum(orbs), self._norb))
+            spec = (orbs, sg)
+        old = self._gas
+        same = (old is None and spec is None) or (
+            old is not None and spec is not None and old[0] == spec[0] and np.array_equal(old[1], spec[1]))
+        if same:
+            return
+        self._gas = spec
+        self._symcache = {}
+        self.confgas = None if spec is None else make_confgas(
+            self._norb, self._neleca, self._nelecb, self.econf_det_mask, spec)
+
+    def _conf_selected(self):
+        """Boolean device mask over configurations: those of irrep wfnsym
+        (with point-group symmetry) and inside the GAS restriction (with
+        one); None when neither restricts the space."""
+        sym = self.wfnsym is not None and self._orbsym is not None
+        if not sym and self._gas is None:
             return None
-        w = int(self.wfnsym)
-        st = self._symcache.get(w)
+        sel = None
+        if sym:
+            sel = self.confsym == int(self.wfnsym)
+        if self._gas is not None:
+            g = self.confgas.to(torch.bool)
+            sel = g if sel is None else (sel & g)
+        return sel
+
+    def _sym(self):
+        """Packing of the CSF vector to the CSFs of the selected
+        configurations -- those of irrep wfnsym (csfstring.py:74-88) and,
+        with a GAS restriction, inside it: per block the selected
+        configurations and their packed offsets.  None when the space is not
+        restricted."""
+        sym = self.wfnsym is not None and self._orbsym is not None
+        if not sym and self._gas is None:
+            return None
+        key = (int(self.wfnsym) if sym else None, self._gas is not None)
+        st = self._symcache.get(key)
         if st is not None:
             return st
-        cs = self.confsym
+        cs = self._conf_selected()
         sel, offs, nsel = [], [], []
         c0 = 0
         packed = 0
         for b in self._blocks:
             nconf = b["nconf"]
-            idx = torch.nonzero(cs[c0:c0 + nconf] == w).reshape(-1).to(torch.int32)
+            idx = torch.nonzero(cs[c0:c0 + nconf]).reshape(-1).to(torch.int32)
             sel.append(idx.contiguous())
             offs.append(packed)
             nsel.append(int(idx.numel()))
             packed += int(idx.numel()) * b["ncsf"]
             c0 += nconf
-        idx_sym = cs[self.econf_csf_mask.long()] == w
+        idx_sym = cs[self.econf_csf_mask.long()]
         st = dict(sel=sel, offs=offs, nsel=nsel, ncsf=packed, idx_sym=idx_sym,
                   pos=torch.cumsum(idx_sym.to(torch.int64), 0) - 1)
-        self._symcache[w] = st
+        self._symcache[key] = st
         return st
 
     @property
@@ -469,9 +519,10 @@ class CSFTransformer:
         return self._unpack(csfvec, self.idx_sym, order, self._ncsf)
 
     def _idx_sym_det(self):
-        if self.wfnsym is None or self._orbsym is None:
+        cs = self._conf_selected()
+        if cs is None:
             return None
-        return self.confsym[self.econf_det_mask.long()] == int(self.wfnsym)
+        return cs[self.econf_det_mask.long()]
 
     def pack_det(self, detvec, order='C'):
         """csfstring.py:88-96: determinant vector(s) -> the determinants whose
@@ -590,6 +641,22 @@ def make_confsym(norb, neleca, nelecb, econf_det_mask, orbsym):
     confsym = torch.zeros(nconf, dtype=torch.int64, device=dev)
     confsym[econf_det_mask.long()] = detsym
     return confsym
+
+
+def make_confgas(norb, neleca, nelecb, econf_det_mask, gas):
+    """Per configuration, 1 when its total occupation per GAS subspace is one
+    of the supergroups of gas = (subspace sizes, supergroup rows), else 0
+    (csffci_gas_conf_mask), as a device uint8 tensor indexed by
+    configuration."""
+    orbs, sg = gas
+    dev = econf_det_mask.device
+    nconf = int(econf_det_mask.max().item()) + 1 if econf_det_mask.numel() else 0
+    out = torch.zeros(max(nconf, 1), dtype=torch.uint8, device=dev)
+    norbs = np.ascontiguousarray(orbs, dtype=np.int32)
+    rows = np.ascontiguousarray(sg, dtype=np.int32)
+    _capi.call("csffci_gas_conf_mask", norb, neleca, nelecb, ptr(econf_det_mask), len(orbs),
+               norbs.ctypes.data, rows.shape[0], rows.ctypes.data, ptr(out), stream())
+    return out[:nconf]
 
 
 def make_econf_csf_mask(norb, neleca, nelecb, smult):

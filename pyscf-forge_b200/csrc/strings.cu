@@ -2,6 +2,8 @@
 // (configuration-spin-determinant) permutation, configuration masks and the
 // genealogical spin eigenvectors.  All results are bit-exact with the
 // reference (see the citations on each kernel).
+#include <algorithm>
+#include <vector>
 #include <string.h>
 
 #include <string>
@@ -87,6 +89,53 @@ __global__ void k_link_table(int norb, int nelec, unsigned long long nstr, int n
         row[k++] = e;
       }
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// GAS configuration filter
+// ---------------------------------------------------------------------------
+
+// The spin-free supergroups of a GAS restriction as sorted 64-bit keys
+// (6 bits of total occupation per subspace, subspace g at bit 6g) and the
+// orbital mask of each subspace (consecutive orbitals in subspace order).
+constexpr int kGasMaxSpaces = 10;
+constexpr int kGasMaxKeys = 1024;
+struct GasKeys {
+  int ngas, nkey;
+  unsigned long long orbmask[kGasMaxSpaces];
+  unsigned long long key[kGasMaxKeys];
+};
+
+// conf_ok[econf_det_mask[I]] = 1 when the total occupation per subspace of
+// determinant I (alpha + beta) is one of the supergroups; every determinant
+// of a configuration has the same occupations, so the writes of one
+// configuration agree.
+__global__ void k_gas_conf(int norb, int neleca, int nelecb, unsigned long long nb, unsigned long long ndet,
+                           const uint32_t* __restrict__ econf_det_mask, GasKeys K, uint8_t* conf_ok) {
+  __shared__ unsigned long long skey[kGasMaxKeys];
+  for (int i = threadIdx.x; i < K.nkey; i += blockDim.x) skey[i] = K.key[i];
+  __syncthreads();
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < ndet;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long ia = i / nb, ib = i - ia * nb;
+    const unsigned long long sa = str_unrank(norb, neleca, ia), sb = str_unrank(norb, nelecb, ib);
+    unsigned long long key = 0;
+    for (int g = 0; g < K.ngas; ++g)
+      key |= (unsigned long long)(__popcll(sa & K.orbmask[g]) + __popcll(sb & K.orbmask[g])) << (6 * g);
+    int lo = 0, hi = K.nkey - 1;
+    bool ok = false;
+    while (lo <= hi) {
+      const int mid = (lo + hi) >> 1;
+      const unsigned long long v = skey[mid];
+      if (v == key) {
+        ok = true;
+        break;
+      }
+      if (v < key) lo = mid + 1;
+      else hi = mid - 1;
+    }
+    conf_ok[econf_det_mask[i]] = ok ? 1 : 0;
   }
 }
 
@@ -377,6 +426,47 @@ int csffci_link_table(int norb, int nelec, csffci_link_t* link, cudaStream_t str
   if (nlink == 0) return CSFFCI_OK;
   k_link_table<<<grid_for((long long)n, 128), 128, 0, stream>>>(norb, nelec, n, nlink, link);
   return check_launch("link_table");
+}
+
+int csffci_gas_conf_mask(int norb, int neleca, int nelecb, const uint32_t* econf_det_mask, int ngas,
+                         const int32_t* gas_norb, int nsupergroup, const int32_t* supergroups, uint8_t* conf_ok,
+                         cudaStream_t stream) {
+  CSF_REQUIRE(norb >= 1 && norb <= 63 && neleca >= 0 && nelecb >= 0 && neleca <= norb && nelecb <= norb,
+              "gas_conf_mask: bad (norb=%d, nelec=(%d,%d))", norb, neleca, nelecb);
+  CSF_REQUIRE(econf_det_mask && conf_ok && gas_norb && supergroups, "gas_conf_mask: NULL pointer");
+  CSF_REQUIRE(ngas >= 1 && ngas <= kGasMaxSpaces, "gas_conf_mask: ngas=%d outside [1,%d]", ngas, kGasMaxSpaces);
+  CSF_REQUIRE(nsupergroup >= 1 && nsupergroup <= kGasMaxKeys, "gas_conf_mask: %d supergroups outside [1,%d]",
+              nsupergroup, kGasMaxKeys);
+  GasKeys K;
+  K.ngas = ngas;
+  int start = 0;
+  for (int g = 0; g < ngas; ++g) {
+    CSF_REQUIRE(gas_norb[g] >= 1 && start + gas_norb[g] <= norb, "gas_conf_mask: subspace %d does not fit", g);
+    K.orbmask[g] = (gas_norb[g] == 64 ? ~0ull : ((1ull << gas_norb[g]) - 1ull)) << start;
+    start += gas_norb[g];
+  }
+  CSF_REQUIRE(start == norb, "gas_conf_mask: subspaces hold %d of %d orbitals", start, norb);
+  std::vector<unsigned long long> keys((size_t)nsupergroup);
+  for (int r = 0; r < nsupergroup; ++r) {
+    unsigned long long k = 0;
+    for (int g = 0; g < ngas; ++g) {
+      const int n = supergroups[(size_t)r * ngas + g];
+      CSF_REQUIRE(n >= 0 && n <= 2 * gas_norb[g], "gas_conf_mask: occupation %d of subspace %d", n, g);
+      k |= (unsigned long long)n << (6 * g);
+    }
+    keys[(size_t)r] = k;
+  }
+  std::sort(keys.begin(), keys.end());
+  keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+  K.nkey = (int)keys.size();
+  for (int i = 0; i < K.nkey; ++i) K.key[i] = keys[(size_t)i];
+  const unsigned long long na = host_binom(norb, neleca), nb = host_binom(norb, nelecb);
+  const unsigned long long ndet = na * nb;
+  CSF_REQUIRE(ndet <= 0xffffffffull, "gas_conf_mask: %llu determinants exceed uint32 addressing", ndet);
+  if (ndet == 0) return CSFFCI_OK;
+  k_gas_conf<<<grid_for((long long)ndet, 256, 148 * 16), 256, 0, stream>>>(norb, neleca, nelecb, nb, ndet,
+                                                                            econf_det_mask, K, conf_ok);
+  return check_launch("gas_conf_mask");
 }
 
 int csffci_csd_masks(int norb, int neleca, int nelecb, int smult, uint32_t* csd_mask,

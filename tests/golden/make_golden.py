@@ -233,6 +233,52 @@ def c1_case():
     print("C1: %.1fs -> %s  E=%s" % (time.time() - t0, path, e))
 
 
+def gas_case(tag, norb, nelec, gas_orbs, gas_restr, gas_restr_type, rank, smults, nroots=2):
+    """The reference's GAS determinant solver (pyscf/mcscf/fci_gas.py and its
+    C kernels) on the stand-in: the canonical spin-supergroups of the
+    restriction (addons_gas.normalize_gas_spec), the allowed determinants in
+    full-CAS order (fci_gas.gas2fci), and the spectrum of the GAS Hamiltonian
+    (the reference's GAS sigma applied to unit vectors) with <S^2> of every
+    eigenvector (the reference's GAS spin_square).  The golden energies of a
+    spin multiplicity are the lowest eigenvalues whose <S^2> is S(S+1)."""
+    from pyscf.mcscf import addons_gas, fci_gas
+    t0 = time.time()
+    h1, eri = seeded_integrals(norb, rank)
+    kernel_orbs, blocks = addons_gas.normalize_gas_spec(gas_orbs, nelec, gas_restr, gas_restr_type)
+    solver = fci_gas.FCISolver(gas_orbs=gas_orbs, gas_restr=gas_restr, gas_restr_type=gas_restr_type)
+    h2e = fci_gas.absorb_h1e(h1, eri, norb, nelec, fac=0.5)
+    with solver.make_space(norb, nelec, compress_links=True) as gas:
+        ndet = gas.ndet
+        allowed = fci_gas.gas2fci(np.ones(ndet), gas) != 0
+        with fci_gas.GasContractPlan(gas, h2e) as plan:
+            H = np.empty((ndet, ndet))
+            unit = np.zeros(ndet)
+            for i in range(ndet):
+                unit[i] = 1.0
+                H[:, i] = plan.contract(unit)
+                unit[i] = 0.0
+    e, v = np.linalg.eigh(0.5 * (H + H.T))
+    s2 = np.array([solver.spin_square(v[:, k], norb, nelec)[0] for k in range(ndet)])
+    out = dict(norb=norb, neleca=nelec[0], nelecb=nelec[1], h1=h1, eri=eri,
+               gas_orbs=np.asarray(gas_orbs), kernel_gas_orbs=np.asarray(kernel_orbs),
+               blocks=np.asarray(blocks), allowed_dets=allowed, spectrum=e, spectrum_s2=s2,
+               smults=np.asarray(smults), nroots=nroots, gas_restr_type=gas_restr_type)
+    if isinstance(gas_restr, dict):
+        out["ras_max_holes"] = gas_restr["max_holes"]
+        out["ras_max_particles"] = gas_restr["max_particles"]
+    else:
+        out["gas_restr"] = np.asarray(gas_restr)
+    for sm in smults:
+        ss = 0.25 * (sm - 1) * (sm + 1)
+        sel = np.nonzero(np.abs(s2 - ss) < 1e-6)[0][:nroots]
+        out["energies_s%d" % sm] = e[sel]
+    path = os.path.join(HERE, "%s.npz" % tag)
+    np.savez_compressed(path, **out)
+    print("%s: ndet_gas=%d nblock=%d  %.1fs -> %s  E=%s" % (
+        tag, ndet, len(blocks), time.time() - t0, path,
+        {sm: out["energies_s%d" % sm] for sm in smults}))
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--c1", action="store_true")
@@ -249,5 +295,11 @@ if __name__ == "__main__":
     symm_case("symm_norb7_4e3e_s12_w1", 7, (4, 3), 2, 12, [0, 1, 0, 1, 3, 2, 0], 1, nroots=2)
     symm_case("symm_norb6_3e3e_s1_w3", 6, (3, 3), 3, 10, [0, 1, 2, 3, 0, 1], 3, nroots=1)
     spin_case()
+    gas_case("gas_ras_norb6_3e3e", 6, (3, 3), (2, 2, 2), {"max_holes": 1, "max_particles": 1}, "ras", 8, (1, 3))
+    gas_case("gas_cumocc_norb7_4e3e", 7, (4, 3), (3, 2, 2), [[4, 6], [6, 7], [7, 7]], "cumulative-occ", 10,
+             (2, 4))
+    gas_case("gas_supergroup_norb6_3e3e", 6, (3, 3), (3, 3), [[4, 2], [3, 3], [5, 1]], "supergroup", 8, (1, 3))
+    gas_case("gas_spinsg_norb6_2e2e", 6, (2, 2), (2, 4),
+             [[1, 1, 1, 1], [2, 0, 0, 2], [0, 2, 2, 0], [1, 1, 0, 2], [0, 2, 1, 1]], "spin-supergroup", 8, (1, 3))
     if args.c1:
         c1_case()

@@ -157,3 +157,50 @@ def test_symmetric_energies_against_dense_csf_hamiltonian(tag):
     w = np.linalg.eigvalsh(Us @ H @ Us.T)
     e = np.atleast_1d(g["energies"])
     np.testing.assert_allclose(w[:e.size], e, atol=1e-9)
+
+
+GAS_CASES = ["gas_ras_norb6_3e3e", "gas_cumocc_norb7_4e3e", "gas_supergroup_norb6_3e3e", "gas_spinsg_norb6_2e2e"]
+
+
+@pytest.mark.parametrize("tag", GAS_CASES)
+def test_gas_membership_restatement_matches_reference(tag):
+    """The determinants of the reference's GAS space (fci_gas.gas2fci of its
+    canonical blocks) equal the restated membership rule bit for bit, and
+    form whole configurations (the spin-complete sets the CSF solver
+    takes)."""
+    g = load_golden(tag)
+    norb, na, nb = int(g["norb"]), int(g["neleca"]), int(g["nelecb"])
+    allowed = R.gas_allowed_dets(norb, na, nb, g["kernel_gas_orbs"].tolist(), g["blocks"])
+    np.testing.assert_array_equal(allowed, g["allowed_dets"])
+    econf = R.make_econf_det_mask(norb, na, nb, R.make_csd_mask(norb, na, nb))
+    R.make_confgas(econf, allowed)
+
+
+@pytest.mark.parametrize("tag", GAS_CASES)
+def test_gas_energies_against_dense_csf_hamiltonian(tag):
+    """The CSF solver's GAS restriction is a filter on configurations: the
+    dense CSF-basis Hamiltonian restricted to the CSFs of the allowed
+    configurations (reference GAS sigma on unit vectors, restated
+    transforms) has, for each spin, the lowest eigenvalues that the
+    reference's GAS determinant Hamiltonian gives that spin (1e-9 Eh)."""
+    if not gasref.available():
+        pytest.skip("reference library not built")
+    g = load_golden(tag)
+    norb, na, nb = int(g["norb"]), int(g["neleca"]), int(g["nelecb"])
+    h2e = R.absorb_h1e(g["h1"], g["eri"], norb, (na, nb), 0.5)
+    nsa, nsb = R.num_strings(norb, na), R.num_strings(norb, nb)
+    ndet = nsa * nsb
+    H = np.empty((ndet, ndet))
+    for i in range(ndet):
+        e = np.zeros(ndet)
+        e[i] = 1.0
+        H[:, i] = gasref.contract_2e(h2e, e.reshape(nsa, nsb), norb, (na, nb)).ravel()
+    econf = R.make_econf_det_mask(norb, na, nb, R.make_csd_mask(norb, na, nb))
+    confok = R.make_confgas(econf, g["allowed_dets"])
+    for sm in g["smults"].tolist():
+        idx = confok[R.make_econf_csf_mask(norb, na, nb, sm)]
+        U = R.transform_det2csf(np.eye(idx.size), norb, na, nb, sm, reverse=True)
+        Us = U[idx]
+        w = np.linalg.eigvalsh(Us @ H @ Us.T)
+        e = g["energies_s%d" % sm]
+        np.testing.assert_allclose(w[:e.size], e, atol=1e-9)
