@@ -440,19 +440,31 @@ class CSFFCISolver:
         h2e = direct_spin1.dev_absorb_h1e(h1e_c, eri_pair_matrix(eri, norb), norb, nelec, fac)
         return H2eff(h2e, h1e_s)
 
-    def contract_2e(self, eri, fcivec, norb, nelec, link_index=None, **kwargs):
+    def contract_2e(self, eri, fcivec, norb, nelec, link_index=None, out=None, **kwargs):
+        """csf.py:521-529.  out (optional, a contiguous float64 torch tensor
+        with fcivec's size, on the device or in host memory) receives the
+        result, which is then returned: a caller that reuses a pinned host
+        buffer gets the result with one DMA copy and no allocation."""
         nelec = _unpack_nelec(nelec)
         if isinstance(eri, H2eff):
             h2e, h1e_s = eri.h2e, eri.h1e_s
         else:
             h2e, h1e_s = to_dev(eri_pair_matrix(eri, norb)), None
         ci = to_dev(fcivec).reshape(-1)
+        if out is not None and (not isinstance(out, torch.Tensor) or out.numel() != ci.numel()
+                                or out.dtype != torch.float64 or not out.is_contiguous()):
+            raise ValueError("out must be a contiguous float64 torch tensor of the CI vector's size")
         eta = None
         if nelec[0] == nelec[1]:
             eta = direct_spin1.dev_spin_parity(ci, comb(norb, nelec[0]))
-        hc = direct_spin1.dev_contract_2e(h2e, ci, norb, nelec, eta=eta)
+        dev_out = out.reshape(-1) if out is not None and out.is_cuda else None
+        hc = direct_spin1.dev_contract_2e(h2e, ci, norb, nelec, eta=eta, out=dev_out)
         if h1e_s is not None:
             direct_spin1.dev_contract_1e(h1e_s, -h1e_s, ci, norb, nelec, hc)
+        if out is not None:
+            if not out.is_cuda:
+                out.reshape(-1).copy_(hc)
+            return out
         shape = fcivec.shape if hasattr(fcivec, "shape") else np.shape(fcivec)
         return like_input(hc.reshape(shape), fcivec)
 

@@ -371,3 +371,35 @@ def test_sigma_kernels_agree(norb, nelec, smult):
         h2e_np = h2e.cpu().numpy()
         np.testing.assert_allclose(got.cpu().numpy(), gasref.contract_2e(h2e_np, c.cpu().numpy(), norb, nelec),
                                    atol=1e-10)
+
+
+@needs_ref
+def test_solver_contract_2e_out_buffers():
+    """FCISolver.contract_2e: numpy in/out, pinned host in with the result
+    in pinned host memory, out= into a reused pinned host buffer and into a
+    device buffer -- all equal to the reference C sigma; a wrong out is a
+    ValueError."""
+    import pyscf_forge_b200 as P
+    norb, nelec = 8, (4, 4)
+    h1, eri = seeded_integrals(norb, 12, seed=7)
+    sol = P.csf_solver(None, smult=1)
+    h2eff = sol.absorb_h1e(h1, eri, norb, nelec, 0.5)
+    rng = np.random.default_rng(8)
+    n = R.num_strings(norb, nelec[0])
+    c = rng.normal(size=(n, n))
+    c = (c + c.T) / np.linalg.norm(c + c.T)  # singlet-symmetric: the row-local singlet kernel runs
+    ref = gasref.contract_2e(R.absorb_h1e(h1, eri, norb, nelec, 0.5), c, norb, nelec).ravel()
+    got = sol.contract_2e(h2eff, c, norb, nelec)
+    np.testing.assert_allclose(np.asarray(got).ravel(), ref, atol=1e-10)
+    ch = torch.from_numpy(c.ravel().copy()).pin_memory()
+    r1 = sol.contract_2e(h2eff, ch, norb, nelec)
+    assert r1.device.type == "cpu" and r1.is_pinned()
+    np.testing.assert_allclose(r1.numpy(), ref, atol=1e-10)
+    buf = torch.empty(n * n, dtype=torch.float64).pin_memory()
+    assert sol.contract_2e(h2eff, ch, norb, nelec, out=buf) is buf
+    np.testing.assert_allclose(buf.numpy(), ref, atol=1e-10)
+    dbuf = torch.empty(n * n, dtype=torch.float64, device="cuda")
+    assert sol.contract_2e(h2eff, ch, norb, nelec, out=dbuf) is dbuf
+    np.testing.assert_allclose(dbuf.cpu().numpy(), ref, atol=1e-10)
+    with pytest.raises(ValueError):
+        sol.contract_2e(h2eff, ch, norb, nelec, out=torch.empty(n * n - 1, dtype=torch.float64))
