@@ -44,10 +44,11 @@ METRIC = "CAS(16,16) FP64 sigma/s"
 WORKLOADS = {"cas16": (16, (8, 8), 32), "cas14": (14, (7, 7), 28), "cas12": (12, (6, 6), 24)}
 
 
-# DRAM bytes (read + write) per k_sigma_rr launch from one ncu capture of
-# the full-size launch (profiles/k_sigma_rr_cas16_dram.md); None for the
-# profiling workloads that were not captured at full size
-TRAFFIC = {"cas16": 26934597120 + 13410886400}
+# DRAM bytes (read + write) per sigma launch, by (workload, kernel), from
+# one ncu capture of the full-size launch (profiles/k_sigma_*_cas16_dram.md);
+# None for what was not captured at full size
+TRAFFIC = {("cas16", "k_sigma_rr"): 26934597120 + 13410886400,
+           ("cas16", "k_sigma_ws"): 30418387968 + 15770089216}
 
 
 def seeded_integrals(norb, rank, seed=0):
@@ -244,7 +245,6 @@ def run_ours(args, rank_env):
     del x
     out = torch.empty_like(c)
     ndet, B, F = algorithmic(NORB, NELEC)
-    traffic = TRAFFIC.get(args.workload)
 
     def step():
         D.dev_contract_2e(h2eff.h2e, c, NORB, NELEC, eta=eta, out=out)
@@ -272,7 +272,9 @@ def run_ours(args, rank_env):
     ms = e0.elapsed_time(e1) / args.steps
     ms = max_over_ranks(ms, world)
     value = world * 1000.0 / ms
-    k_cnt, k_ms = prof.get("k_sigma_rr", prof.get("k_sigma", (0, 0.0)))
+    kname = next((k for k in ("k_sigma_ws", "k_sigma_rr", "k_sigma") if k in prof), "k_sigma_rr")
+    k_cnt, k_ms = prof.get(kname, (0, 0.0))
+    traffic = TRAFFIC.get((args.workload, kname))
     k_avg_ms = k_ms / max(k_cnt, 1)
     launches = sum(v[0] for v in prof.values())
 
@@ -315,7 +317,7 @@ def run_ours(args, rank_env):
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic,
-                         "kernel": "k_sigma_rr" if "k_sigma_rr" in prof else "k_sigma",
+                         "kernel": kname,
                          "algorithmic_bytes": B,
                          "flops": F, "tflops": F / (k_avg_ms * 1e-3) / 1e12,
                          "flops_formed": F / 2, "dmma_peak_tflops": dmma,

@@ -51,6 +51,20 @@ static const int kVariantShape[RR_NVARIANT][2] = {{16, 4}, {8, 4}, {16, 2}, {8, 
 
 bool rr_variant_valid(int norb, int v) { return v >= 0 && v < RR_NVARIANT && !(v == 0 && norb >= 15); }
 
+// one problem: the warp-specialised kernel from 14 orbitals (CSFFCI_SIGMA_VARIANT
+// may name any variant); -1 leaves the choice to rr_default_variant
+static int rr_single_variant(int norb) {
+  const char* env = getenv("CSFFCI_SIGMA_VARIANT");
+  if (env) {
+    const int v = atoi(env);
+    if (v == RR_VARIANT_WS && sigma_ws_supported(norb)) return RR_VARIANT_WS;
+    if (rr_variant_valid(norb, v)) return v;
+  }
+  // measured on B200 (singlet, one problem): 14 orbitals 7.61 -> 6.31 ms,
+  // 15: 31.1 -> 25.8 ms, 16: 148.8 -> 139.6 ms; at 13 it is no faster
+  return norb >= 14 && sigma_ws_supported(norb) ? RR_VARIANT_WS : -1;
+}
+
 int rr_default_variant(int norb) {
   const char* env = getenv("CSFFCI_SIGMA_VARIANT");
   if (env) {
@@ -91,7 +105,15 @@ int sigma_rr_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev,
                     int max_nla, int max_nlb, cudaStream_t stream, int variant) {
   const int npair = norb * (norb + 1) / 2;
   const int ks = (npair + 3) / 4;
+  if (variant < 0 && !jobs_dev) variant = rr_single_variant(norb);
   if (variant < 0) variant = rr_default_variant(norb);
+  if (variant == RR_VARIANT_WS) {
+    if (jobs_dev) {
+      set_error("sigma: the warp-specialised variant takes one problem, not a job table");
+      return CSFFCI_ERR_INVALID;
+    }
+    return sigma_ws_launch(norb, job0, total_units, max_nb, max_nla, max_nlb, stream);
+  }
   if (!rr_variant_valid(norb, variant)) {
     set_error("sigma: tile variant %d is not available for norb=%d", variant, norb);
     return CSFFCI_ERR_INVALID;

@@ -29,6 +29,7 @@ struct RRArgs {
   long long total_units;
   int npair, ds, ls, nd_rows;
   unsigned off_d, off_l, off_crow, off_al, off_zl, off_pn, off_zf;
+  unsigned off_ap;  // warp-specialised kernel: per-pair alpha offsets
 };
 
 // Alpha link of the current row Ja as the tile loops use it: the offset
@@ -412,6 +413,11 @@ static int launch_rr(RRArgs& g, size_t smem, cudaStream_t stream) {
 
 // tile-shape variants: (rows per warp, n-tiles of 8 columns)
 constexpr int RR_NVARIANT = 4;
+// the warp-specialised kernel (sigma_ws.cu), one problem at 13..16 orbitals
+constexpr int RR_VARIANT_WS = 4;
+bool sigma_ws_supported(int norb);
+int sigma_ws_launch(int norb, const csffci_sigma_job_t& job0, long long total_units, long long max_nb,
+                    int max_nla, int max_nlb, cudaStream_t stream);
 bool rr_variant_valid(int norb, int v);
 int rr_default_variant(int norb);
 int sigma_rr_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev, const csffci_sigma_job_t& job0,

@@ -403,3 +403,36 @@ def test_solver_contract_2e_out_buffers():
     np.testing.assert_allclose(dbuf.cpu().numpy(), ref, atol=1e-10)
     with pytest.raises(ValueError):
         sol.contract_2e(h2eff, ch, norb, nelec, out=torch.empty(n * n - 1, dtype=torch.float64))
+
+
+@needs_ref
+@pytest.mark.parametrize("norb,nelec,rank", [(14, (3, 3), 10), (14, (3, 2), 10), (15, (4, 3), 10),
+                                             (16, (2, 2), 8), (13, (3, 3), 8)])
+def test_warp_specialised_sigma(norb, nelec, rank, monkeypatch):
+    """The warp-specialised sigma kernel (tile variant 4, the single-problem
+    default from 14 orbitals): against the reference C (1e-10) and against
+    the phase-serial kernel (1e-12), in the general and, for na == nb, the
+    spin-symmetric mode."""
+    import torch
+    _, D, _ = _mods()
+    from math import comb
+    h1, eri = seeded_integrals(norb, rank, seed=11)
+    h2e_np = R.absorb_h1e(h1, eri, norb, nelec, 0.5)
+    h2e = torch.as_tensor(h2e_np, device="cuda")
+    na, nb = comb(norb, nelec[0]), comb(norb, nelec[1])
+    rng = np.random.default_rng(12)
+    c = rng.normal(size=(na, nb))
+    if na == nb:
+        c = c + c.T
+    c /= np.linalg.norm(c)
+    ref = gasref.contract_2e(h2e_np, c, norb, nelec).ravel()
+    cd = torch.as_tensor(c.ravel(), device="cuda")
+    etas = (None, 1) if na == nb else (None,)
+    for eta in etas:
+        monkeypatch.setenv("CSFFCI_SIGMA_VARIANT", "4")
+        ws = D.dev_contract_2e(h2e, cd, norb, nelec, eta=eta).cpu().numpy()
+        monkeypatch.setenv("CSFFCI_SIGMA_VARIANT", "1")
+        rr = D.dev_contract_2e(h2e, cd, norb, nelec, eta=eta).cpu().numpy()
+        np.testing.assert_allclose(ws, ref, atol=1e-10)
+        np.testing.assert_allclose(ws, rr, atol=1e-12)
+    monkeypatch.delenv("CSFFCI_SIGMA_VARIANT")
