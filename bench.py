@@ -48,7 +48,7 @@ WORKLOADS = {"cas16": (16, (8, 8), 32), "cas14": (14, (7, 7), 28), "cas12": (12,
 # one ncu capture of the full-size launch (profiles/k_sigma_*_cas16_dram.md);
 # None for what was not captured at full size
 TRAFFIC = {("cas16", "k_sigma_rr"): 26934597120 + 13410886400,
-           ("cas16", "k_sigma_ws"): 30418387968 + 15770089216}
+           ("cas16", "k_sigma_ws"): 33107436032 + 16856211456}
 
 
 def seeded_integrals(norb, rank, seed=0):

@@ -61,7 +61,7 @@ static int rr_single_variant(int norb) {
     if (rr_variant_valid(norb, v)) return v;
   }
   // measured on B200 (singlet, one problem): 14 orbitals 7.61 -> 6.31 ms,
-  // 15: 31.1 -> 25.8 ms, 16: 148.8 -> 139.6 ms; at 13 it is no faster
+  // 15: 31.1 -> 25.8 ms, 16: 148.8 -> 129.5 ms; at 13 it is no faster
   return norb >= 14 && sigma_ws_supported(norb) ? RR_VARIANT_WS : -1;
 }
 

@@ -27,9 +27,8 @@
 // fragments are not held in the movers' code.
 //
 // The CTA has a multiple of four warps, so every scheduler gets the same
-// number; at 16 orbitals that is 18 MMA warps (the 17th m-tile split over
-// two warps) and 2 movers, 5 warps per scheduler: the register budget of
-// k_sigma_rr, which the A fragments need.
+// number; at 16 orbitals that is 17 MMA warps and 3 movers, 5 warps per
+// scheduler: the register budget of k_sigma_rr, which the A fragments need.
 #include <stdlib.h>
 
 #include "sigma_rr_kernel.cuh"
@@ -59,8 +58,13 @@ __device__ __forceinline__ void ws_dmma(double& c0, double& c1, double a, double
 template <int MT>
 struct WSLayout {
   static constexpr int q = MT / 4, r = MT % 4;
-  static constexpr bool split = q >= 1 && (r == 1 || r == 2);
-  static constexpr int NWM = split ? 4 * q + 2 * r : MT;
+  // splitting balances the MMA units over the schedulers; it is skipped
+  // where it would leave fewer than three movers (17 m-tiles: 18 MMA warps
+  // and 2 movers against 17 and 3), the movers being the limit there
+  static constexpr bool split0 = q >= 1 && (r == 1 || r == 2);
+  static constexpr int NWM0 = split0 ? 4 * q + 2 * r : MT;
+  static constexpr bool split = split0 && 4 * ((NWM0 + 2 + 3) / 4) - NWM0 >= 3;
+  static constexpr int NWM = split ? NWM0 : MT;
   static constexpr int NTOT = 4 * ((NWM + 2 + 3) / 4);
   static constexpr int NMOV = NTOT - NWM;
 };
