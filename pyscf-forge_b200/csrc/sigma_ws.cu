@@ -276,7 +276,6 @@ __global__ void __launch_bounds__(WSLayout<MT>::NTOT * 32, 1) k_sigma_ws(RRArgs 
         const int nch = srow.nchunk;
         const long long jend = srow.jend, ja = srow.ja, Nb = sjob.Nb;
         const int nla = sjob.nla, nlb = sjob.nlb, nz = srow.nzero;
-        (void)ja;
         const unsigned* pc = S.pneg + srow.pc;
         const bool SYM = sjob.sym != 0;
         double* const out = SYM ? sjob.scratch : sjob.sigma;
