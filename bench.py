@@ -45,8 +45,8 @@ WORKLOADS = {"cas16": (16, (8, 8), 32), "cas14": (14, (7, 7), 28), "cas12": (12,
 
 
 # DRAM bytes (read + write) per sigma launch, by (workload, kernel), from
-# one ncu capture of the full-size launch (profiles/k_sigma_*_cas16_dram.md);
-# None for what was not captured at full size
+# one ncu capture of the dram byte counters on the full-size launch; None
+# for what was not captured
 TRAFFIC = {("cas16", "k_sigma_rr"): 26934597120 + 13410886400,
            ("cas16", "k_sigma_ws"): 33107436032 + 16856211456}
 
@@ -148,17 +148,8 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference_sigma(norb, nelec, rank, budget_s=25.0, min_steps=1):
-    """Time the reference's own CPU sigma (fci_contract_gas_plan_execute,
-    pyscf/lib/mcscf/fci_contract_gas.c:2423) on all host threads.  Returns
-    (sigma/s, cores, sample description)."""
-    import numpy as np
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import gasref
-    import restate as R
+def _cpu_info():
     cores = len(os.sched_getaffinity(0))
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    from math import comb
     cpu_model = ""
     try:
         for ln in open("/proc/cpuinfo"):
@@ -167,51 +158,69 @@ def cpu_reference_sigma(norb, nelec, rank, budget_s=25.0, min_steps=1):
                 break
     except Exception:
         pass
+    return cores, cpu_model
 
-    def timed(no, ne, rk, budget, nmin):
-        h1, eri = seeded_integrals(no, rk)
-        h2e = R.absorb_h1e(h1, eri, no, ne, 0.5)
-        plan = gasref.SigmaPlan(no, ne, h2e)
-        nd = comb(no, ne[0]) * comb(no, ne[1])
-        ci = np.random.default_rng(1).normal(size=nd)
-        ci /= np.linalg.norm(ci)
-        n = 0
-        t0 = time.perf_counter()
-        while True:
-            plan(ci)
-            n += 1
-            el = time.perf_counter() - t0
-            if n >= nmin and (el > budget / 2 or el + el / n > budget):
-                break
-        plan.close()
-        return n, el
 
-    # a CAS(14,14) sigma first; run the full CAS(16,16) sigma when the host
-    # finishes it within the budget, else scale by the flop ratio
-    n14, t14 = timed(14, (7, 7), 28, min(budget_s, 10.0), 1)
-    ratio = algorithmic(norb, nelec)[2] / algorithmic(14, (7, 7))[2]
-    est = t14 / n14 * ratio
-    if est <= budget_s:
-        n, el = timed(norb, nelec, rank, budget_s, min_steps)
-        return n / el, cores, "%d full CAS(%d,%d) sigma(s) in %.1f s on %d threads (%s)" % (
-            n, norb, norb, el, cores, cpu_model)
-    return (n14 / t14) / ratio, cores, (
-        "%d CAS(14,14) (7,7) sigma(s) in %.1f s on %d threads (%s), scaled to CAS(16,16) by the "
-        "flop ratio %.1f (a full CAS(16,16) sigma is estimated at %.0f s here)" % (
-            n14, t14, cores, cpu_model, ratio, est))
+def reference_sigma_plan(norb, nelec, h2e):
+    """The reference's own CPU sigma (fci_contract_gas_plan_create/execute,
+    pyscf/lib/mcscf/fci_contract_gas.c:2388-2452, one GAS subspace = the
+    full CAS) on all host threads.  Used only as the timed CPU baseline and
+    as the checker of the timed GPU output, never on the measured path."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import gasref
+    cores, _ = _cpu_info()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    return gasref.SigmaPlan(norb, nelec, h2e)
+
+
+def bench_config(world):
+    """The workload both arms report (the same dict, so that the two lines
+    describe the same configuration)."""
+    ndet = algorithmic(NORB, NELEC)[0]
+    return {"workload": WORKLOAD, "norb": NORB, "nelec": list(NELEC), "eri_rank": RANK, "ndet": ndet,
+            "vector": "normalised singlet-symmetric CI vector (c = c^T), seeded",
+            "l2": "inputs 1.33 GB >> 126 MB L2 (no flush needed)",
+            "parallelism": "replicas%d" % world}
 
 
 def run_reference(args, rank_env):
+    """Reference arm: the reference's own CPU sigma on the benchmark's
+    workload, on all host threads of rank 0.  One full CAS(16,16) sigma
+    takes tens of seconds, so the arm times as many whole sigmas as fit in
+    about 90 s (at least one, at most --steps) and reports that count as
+    ``steps``; no warm-up is needed for a CPU library call (the plan is
+    built before the timed loop)."""
+    import numpy as np
     rank, world = rank_env
     if rank != 0:
         return
-    value, cores, sample = cpu_reference_sigma(NORB, NELEC, RANK, budget_s=max(30.0, 20.0 * args.steps / 10),
-                                               min_steps=1)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import restate as R
+    from math import comb
+    h1, eri = seeded_integrals(NORB, RANK)
+    h2e = R.absorb_h1e(h1, eri, NORB, NELEC, 0.5)
+    plan = reference_sigma_plan(NORB, NELEC, h2e)
+    n = comb(NORB, NELEC[0])
+    c = np.random.default_rng(1).normal(size=(n, n))
+    c += c.T
+    c /= np.linalg.norm(c)
+    budget = 90.0
+    nsig, t0 = 0, time.perf_counter()
+    while True:
+        plan(c)
+        nsig += 1
+        el = time.perf_counter() - t0
+        if nsig >= max(1, args.steps) or el + el / nsig > budget:
+            break
+    plan.close()
+    value = nsig / el
+    cores, cpu_model = _cpu_info()
+    sample = "%d full CAS(16,16) (8,8) sigma(s) in %.1f s on %d threads (%s)" % (nsig, el, cores, cpu_model)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "sigma/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "norb": NORB, "nelec": list(NELEC), "eri_rank": RANK},
+            "n_gpus": world, "steps": nsig, "warmup": 0, "requested_steps": args.steps,
+            "requested_warmup": args.warmup, "ms_per_step": 1000.0 * el / nsig, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": bench_config(world),
             "cpu_baseline": {"value": value, "unit": "sigma/s", "cores": cores, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": "sigma/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -308,9 +317,7 @@ def run_ours(args, rank_env):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded rank-32 integrals, random singlet CSF vector)",
-            "config": {"workload": WORKLOAD, "norb": NORB, "nelec": list(NELEC), "eri_rank": RANK,
-                       "ndet": ndet, "l2": "inputs 1.33 GB >> 126 MB L2 (no flush needed)",
-                       "parallelism": "replicas%d" % world},
+            "config": bench_config(world),
             "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "sigma/s",
                     "h2d_bytes_per_step": ndet * 8, "d2h_bytes_per_step": ndet * 8,
                     "note": "FCISolver.contract_2e, pinned host vector in, pinned host buffer out (out=)"},
@@ -327,13 +334,31 @@ def run_ours(args, rank_env):
                          "peak_note": "hbm_gbs %s (MEASURED_PEAKS.json)" % src},
             "clocks": clk.summary()}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, cores, sample = cpu_reference_sigma(NORB, NELEC, RANK, budget_s=20.0)
-        line["cpu_baseline"] = {"value": v, "unit": "sigma/s", "cores": cores, "kind": "reference",
-                                "sample": sample}
+        # one full reference sigma on the host, on the very vector the timed
+        # loop used: the measured CPU baseline, and the check of the timed
+        # output against the reference
+        h2e_np = h2eff.h2e.cpu().numpy()
+        c_np = c.cpu().numpy()
+        plan = reference_sigma_plan(NORB, NELEC, h2e_np)
+        t0 = time.perf_counter()
+        ref = plan(c_np)
+        t_ref = time.perf_counter() - t0
+        plan.close()
+        ref_d = torch.as_tensor(ref, device=out.device)
+        del ref, c_np
+        line["max_abs_err_vs_reference"] = float((out - ref_d).abs().max())
+        line["max_abs_sigma"] = float(ref_d.abs().max())
+        del ref_d
+        cores, cpu_model = _cpu_info()
+        line["cpu_baseline"] = {"value": 1.0 / t_ref, "unit": "sigma/s", "cores": cores, "kind": "reference",
+                                "sample": "1 full CAS(16,16) (8,8) sigma of the benchmark's own vector in "
+                                          "%.1f s on %d threads (%s)" % (t_ref, cores, cpu_model)}
     if rank == 0 and world == 1 and not args.no_rdm:
         line["rdm"] = run_rdm(dmma)
     if rank == 0 and world == 1 and not args.no_batched:
         line["batched"] = run_batched(args.batch)
+    if rank == 0 and world == 1 and not args.no_c4:
+        line["c4"] = run_c4(ref_check=not args.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -376,6 +401,84 @@ def run_rdm(dmma_peak, cases=None):
     out["note"] = ("adjoint = transition-density / RDM kernel: T slabs <J|E_pq|c> built in shared memory, "
                    "Gram on FP64 DMMA (bra == ket: symmetric half), 1-RDM from the Gram; flops counted "
                    "as the dense 2*ndet*norb^4")
+    return out
+
+
+def run_c4(ref_check=True):
+    """The large configuration: CAS(16,16) (8,8) singlet, 4 roots
+    state-averaged with equal weights.  The solve is FCISolver.kernel (the
+    reference's kernel, pyscf/csf_fci/csf.py:368-497: CSF diagonal,
+    p-space, Olsen preconditioner, Davidson on hop = csf2det . sigma .
+    det2csf) reached through the differentiable energy; the backward of the
+    state-averaged energy then runs the 1-/2-RDM kernel on every root.
+    Reported: solve and backward seconds, Davidson iterations and sigmas,
+    the device memory peak, device time per kernel, and the checks
+      * |H c_k - E_k c_k| of every root (the library's sigma),
+      * tr dm1 = N and sum_pr dm2[p,p,r,r] = N(N-1) of the averaged RDMs,
+      * E_SA = sum h1 * dE/dh1 + sum eri * dE/deri (H is linear in h1, eri),
+      * with ref_check, <c_0|H|c_0> and |H c_0 - E_0 c_0| with the
+        reference's own CPU sigma on the host."""
+    import numpy as np
+    import torch
+    from pyscf_forge_b200 import _capi
+    from pyscf_forge_b200.autograd import csf_fci_energy
+    from pyscf_forge_b200.csf_fci.csf import FCISolver
+    from pyscf_forge_b200.fci import direct_spin1 as D
+    norb, nelec, rank, nroots = 16, (8, 8), 32, 4
+    h1, eri = seeded_integrals(norb, rank)
+    h1t = torch.tensor(h1, requires_grad=True)
+    erit = torch.tensor(eri, requires_grad=True)
+    sol = FCISolver(None, smult=1)
+    torch.cuda.synchronize()
+    torch.cuda.reset_peak_memory_stats()
+    _capi.profile_enable(True)
+    t0 = time.perf_counter()
+    E = csf_fci_energy(h1t, erit, norb, nelec, smult=1, nroots=nroots, solver=sol)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    w = torch.full((nroots,), 1.0 / nroots, dtype=torch.float64)
+    e_sa = (w * E).sum()
+    e_sa.backward()
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    prof = _capi.profile_report()
+    _capi.profile_enable(False)
+    peak = torch.cuda.max_memory_allocated()
+    gh1, geri = h1t.grad.numpy(), erit.grad.numpy()
+    n = sum(nelec)
+    dm1 = gh1.T
+    dm2 = 2.0 * geri
+    out = {"workload": "CAS(16,16) (8,8) singlet, %d roots state-averaged (equal weights), "
+                       "seeded rank-32 integrals" % nroots,
+           "energies": [float(x) for x in E.detach()], "e_sa": float(e_sa),
+           "converged": [bool(x) for x in np.atleast_1d(sol.converged)],
+           "solve_s": t1 - t0, "rdm_backward_s": t2 - t1, "sigmas": int(getattr(sol, "nsigma", 0)),
+           "davidson_iterations": int(getattr(sol, "niter", 0)),
+           "device_peak_gb": peak / 1e9, "hbm_budget_gb": 180.0,
+           "trace_dm1_minus_n": float(np.trace(dm1) - n),
+           "trace_dm2_minus_n_n1": float(np.einsum("pprr->", dm2) - n * (n - 1)),
+           "energy_from_gradients_minus_e_sa": float(np.sum(h1 * gh1) + np.sum(eri * geri) - float(e_sa)),
+           "kernel_ms": {k: round(v[1], 3) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+           "kernel_launches": {k: v[0] for k, v in prof.items()}}
+    h2e = sol.absorb_h1e(h1, eri, norb, nelec, 0.5).h2e
+    res = []
+    for k, c in enumerate(sol.ci):
+        c = c.reshape(-1)
+        hc = D.dev_contract_2e(h2e, c, norb, nelec)
+        res.append(float(torch.linalg.norm(hc - float(E[k]) * c)))
+        del hc
+    out["residual_norms"] = res
+    if ref_check:
+        import restate as R
+        c0 = sol.ci[0].reshape(-1).cpu().numpy()
+        plan = reference_sigma_plan(norb, nelec, R.absorb_h1e(h1, eri, norb, nelec, 0.5))
+        hc0 = plan(c0)
+        plan.close()
+        e0 = float(np.dot(c0, hc0) / np.dot(c0, c0))
+        out["reference_check_root0"] = {
+            "rayleigh_quotient_minus_e0": e0 - float(E[0]),
+            "residual_norm": float(np.linalg.norm(hc0 - float(E[0]) * c0)),
+            "note": "the reference's CPU sigma (libfci_gas, one GAS subspace) applied to root 0"}
     return out
 
 
@@ -434,6 +537,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="time the device loop only (profiling)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-solves measurement")
     ap.add_argument("--no-rdm", action="store_true", help="skip the RDM (adjoint) timing")
+    ap.add_argument("--no-c4", action="store_true", help="skip the CAS(16,16) 4-root solve + RDM backward")
+    ap.add_argument("--c4-only", action="store_true", help="only the CAS(16,16) 4-root solve + RDM backward")
     ap.add_argument("--rdm-only", default="", help="only the RDM timing of these cases "
                     "(cas16_singlet_1root,cas14_sa2), for profiling captures")
     ap.add_argument("--batch", type=int, default=128, help="problems in the batched-solves measurement")
@@ -442,6 +547,12 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
         run_reference(args, (rank, world))
+        return
+    if args.c4_only:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        if rank == 0:
+            print(json.dumps(run_c4(ref_check=not args.no_cpu_baseline)), flush=True)
         return
     if args.rdm_only:
         # the adjoint timing alone (profiling captures of the RDM kernels)

@@ -176,8 +176,11 @@ int csffci_hdiag_det(int norb, int neleca, int nelecb, const double* h1a,
  * (Na*(norb+1) + 2*Nb doubles; up to norb = 16 at half filling fits) are
  * rejected with CSFFCI_ERR_MEMORY.  The first call on a device looks up
  * the array's device address, so make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU (other
- * streams, other host threads) race and must be serialised by the caller. */
+ * capture; the address is kept per device and context, and the first call
+ * in a new context (after cudaDeviceReset, or under another context made
+ * current) looks it up again.  All calls share the array: calls that
+ * overlap on the GPU (other streams, other host threads) race and must be
+ * serialised by the caller. */
 #define CSFFCI_HDIAG_NOALLOC_MAX_DOUBLES (1 << 18)
 int csffci_hdiag_det_noalloc(int norb, int neleca, int nelecb, const double* h1a,
                              const double* h1b, const double* eri, double* hdiag,
@@ -222,6 +225,34 @@ int csffci_sigma(int norb, int neleca, int nelecb, const double* h2e,
                  const csffci_link_t* link_a, const csffci_link_t* link_b,
                  const double* ci, double* sigma, int flags, int eta, void* work,
                  size_t work_bytes, cudaStream_t stream);
+
+/* Sigma plan: the state of csffci_sigma for one problem bound once, the
+ * model of the reference's contraction plan (fci_contract_gas_plan_create /
+ * _execute / _free, pyscf/lib/mcscf/fci_gas.h:244-253,
+ * fci_contract_gas.c:2388-2452).  create borrows h2e and the link tables
+ * (device pointers that must outlive the plan; their contents are read at
+ * every execute), fixes the sigma kernel for (norb, neleca, nelecb) and
+ * returns the workspace the plan needs (the spin-symmetric scratch when
+ * flags holds CSFFCI_SIGMA_SPIN_SYMMETRIC; flags may also hold
+ * CSFFCI_SIGMA_REFERENCE_KERNEL).  bind hands that workspace over (caller
+ * owned, for the life of the plan).  execute computes sigma from ci on the
+ * stream, with flags ACCUMULATE and/or SPIN_SYMMETRIC (the latter only
+ * when the plan was created with it; eta = +1/-1 as in csffci_sigma); it
+ * allocates nothing and synchronises nothing, so it can be replayed from
+ * a captured graph.  One plan must not be executed concurrently on two
+ * streams (they would share the workspace), as a GAS plan must not be
+ * executed by two host threads at once (fci_gas.h:276-292). */
+typedef struct csffci_sigma_plan csffci_sigma_plan_t;
+int csffci_sigma_plan_create(int norb, int neleca, int nelecb, const double* h2e,
+                             const csffci_link_t* link_a, const csffci_link_t* link_b, int flags,
+                             csffci_sigma_plan_t** plan, size_t* work_bytes);
+int csffci_sigma_plan_bind(csffci_sigma_plan_t* plan, void* work, size_t work_bytes);
+int csffci_sigma_plan_execute(const csffci_sigma_plan_t* plan, const double* ci, double* sigma, int eta,
+                              int flags, cudaStream_t stream);
+/* the kernel the plan runs: 0..3 register-resident tile variants, 4 and 5
+ * the warp-specialised kernels, -2 the shared-memory-h2e kernel */
+int csffci_sigma_plan_variant(const csffci_sigma_plan_t* plan);
+void csffci_sigma_plan_destroy(csffci_sigma_plan_t* plan);
 
 /* One sigma of a batch (csffci_sigma_batch).  The caller fills the first
  * block; the library fills the rest.  sym = 1 asserts neleca == nelecb and

@@ -154,6 +154,11 @@ _SIGS = {
     "csffci_precond_workspace": ([], _sz),
     "csffci_precond": ([_i64, _p, _p, _p, _d, _d, _i, _d, _p, _p, _p], _i),
     "csffci_precond_dots": ([_i64, _p, _p, _p, _d, _d, _p, _p, _p], _i),
+    "csffci_sigma_plan_create": ([_i, _i, _i, _p, _p, _p, _i, ctypes.POINTER(_p), ctypes.POINTER(_sz)], _i),
+    "csffci_sigma_plan_bind": ([_p, _p, _sz], _i),
+    "csffci_sigma_plan_execute": ([_p, _p, _p, _i, _i, _p], _i),
+    "csffci_sigma_plan_variant": ([_p], _i),
+    "csffci_sigma_plan_destroy": ([_p], None),
     "csffci_sigma_batch_workspace": ([_i], _sz),
     "csffci_sigma_batch": ([_i, _i, _p, _p, _sz, _p], _i),
     "csffci_transform_batch": ([_i, _i, _p, _i, _p, _p, _sz, _p], _i),

@@ -80,30 +80,29 @@ def _block_of_conf(transformer):
 def _pspace_transform(transformer, mat, confs):
     """transform_opmat_det2csf_pspace (csfstring.py:676-785): U^T mat U with
     U block-diagonal over the configurations, rows = determinants of the
-    configurations in CSD order, columns = their CSFs (ascending)."""
+    configurations in CSD order, columns = their CSFs (ascending).  U is
+    assembled on the device from the cached spin-eigenvector blocks (one
+    slice copy per configuration), so no block leaves the GPU."""
     confs = np.sort(np.asarray(confs, dtype=np.int64))
     table = _block_of_conf(transformer)
-    rows, cols, vals = [], [], []
+    pieces = []
     det_pos = 0
+    ncol = 0
     csf_addrs = []
     for conf in confs.tolist():
         c0, b = next((c0, b) for (c0, b) in reversed(table) if c0 <= conf)
         local = conf - c0
         nd, nc = b["ndet"], b["ncsf"]
         if nc > 0:
-            u = b["sign"] * b["umat"].cpu().numpy()
-            for i in range(nd):
-                for k in range(nc):
-                    rows.append(det_pos + i)
-                    cols.append(len(csf_addrs) + k)
-                    vals.append(u[i, k])
+            pieces.append((det_pos, ncol, b))
             csf_addrs.extend(range(b["csf_offset"] + local * nc, b["csf_offset"] + (local + 1) * nc))
+            ncol += nc
         det_pos += nd
-    ncsf = len(csf_addrs)
-    U = torch.zeros((det_pos, ncsf), dtype=torch.float64, device=device())
-    if rows:
-        U[torch.as_tensor(rows, device=U.device), torch.as_tensor(cols, device=U.device)] = \
-            torch.as_tensor(vals, dtype=torch.float64, device=U.device)
+    U = torch.zeros((det_pos, ncol), dtype=torch.float64, device=device())
+    for r0, k0, b in pieces:
+        blk = U[r0:r0 + b["ndet"], k0:k0 + b["ncsf"]]
+        blk.copy_(b["umat"])
+        blk.mul_(float(b["sign"]))
     h0 = to_dev(mat)
     Ut = U.T.contiguous()
     Wt = gram(Ut, h0)        # (ncsf, ndet) = U^T h0 (h0 symmetric)
@@ -297,11 +296,13 @@ def kernel(fci, h1e, eri, norb, nelec, smult=None, idx_sym=None, ci0=None, tol=N
         max_space = fci.max_space
     tol_residual = getattr(fci, 'conv_tol_residual', None)
     log = print if getattr(fci, "verbose", 0) >= 5 else None
+    stats = {}
     conv, e, c = davidson(hop, x0, precond, tol=tol, max_cycle=max_cycle, max_space=max_space,
                           lindep=lindep, nroots=nroots, follow_state=True,
-                          tol_residual=tol_residual, log=log)
+                          tol_residual=tol_residual, log=log, stats=stats)
     fci.converged = conv if nroots > 1 else conv[0]
     fci.nsigma = hop.nsigma
+    fci.niter = stats.get("niter", 0)
     fci.kernel_time = time.perf_counter() - t0
     cdet = transformer.dev_csf2det(c)
     cdet = cdet / torch.linalg.norm(cdet, dim=1, keepdim=True)

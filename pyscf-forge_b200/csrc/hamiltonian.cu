@@ -300,7 +300,40 @@ static __device__ __align__(256) double g_hdiag_noalloc_scratch[CSFFCI_HDIAG_NOA
 namespace csffci {
 namespace {
 std::mutex g_noalloc_mutex;
-void* g_noalloc_ptr[256] = {nullptr};  // device address of the array, per device ordinal
+// device address of the array per device ordinal, valid for the context
+// whose unique id is g_noalloc_ctx[dev] (0: not looked up yet)
+void* g_noalloc_ptr[256] = {nullptr};
+unsigned long long g_noalloc_ctx[256] = {0};
+
+// Unique id of the calling thread's current context (cuCtxGetId, reached
+// through the runtime's driver entry points so that libcuda is not linked);
+// 0 when it cannot be had.  Context ids are never reused within a process,
+// so an id that differs from the cached one means the cached address
+// belongs to a context that no longer is current (a cudaDeviceReset, or a
+// context created by another library).
+unsigned long long current_context_id() {
+  typedef int (*get_current_fn)(void**);
+  typedef int (*get_id_fn)(void*, unsigned long long*);
+  static get_current_fn get_current = nullptr;
+  static get_id_fn get_id = nullptr;
+  static bool resolved = false;
+  if (!resolved) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = (get_current_fn)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = (get_id_fn)f;
+    resolved = true;
+  }
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || ctx == nullptr || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
 }  // namespace
 }  // namespace csffci
 
@@ -319,14 +352,15 @@ extern "C" int csffci_hdiag_det_noalloc(int norb, int neleca, int nelecb, const 
     return CSFFCI_ERR_MEMORY;
   }
   // The symbol's name is a host-side stand-in, not a device address: look
-  // the address up once per device, with that device current.
+  // the address up once per device and context, with that device current.
   int dev = 0;
   CSF_CUDA(cudaGetDevice(&dev));
   CSF_REQUIRE(dev >= 0 && dev < 256, "hdiag_det_noalloc: device ordinal %d out of range", dev);
   void* base = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (g_noalloc_ptr[dev] == nullptr) {
+    const unsigned long long ctx = current_context_id();
+    if (g_noalloc_ptr[dev] == nullptr || ctx == 0 || ctx != g_noalloc_ctx[dev]) {
       void* p = nullptr;
       cudaError_t e = cudaGetSymbolAddress(&p, g_hdiag_noalloc_scratch);
       if (e != cudaSuccess || p == nullptr) {
@@ -335,6 +369,7 @@ extern "C" int csffci_hdiag_det_noalloc(int norb, int neleca, int nelecb, const 
         return CSFFCI_ERR_CUDA;
       }
       g_noalloc_ptr[dev] = p;
+      g_noalloc_ctx[dev] = current_context_id();
     }
     base = g_noalloc_ptr[dev];
   }

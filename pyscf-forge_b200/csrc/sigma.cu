@@ -15,6 +15,8 @@
 // cross-row update.
 #include "common.cuh"
 #include "profile.cuh"
+#include <new>
+
 #include "sigma_rr.cuh"
 
 namespace csffci {
@@ -303,9 +305,16 @@ size_t csffci_sigma_workspace(int norb, int neleca, int nelecb, int flags) {
   return 0;
 }
 
-int csffci_sigma(int norb, int neleca, int nelecb, const double* h2e, const csffci_link_t* link_a,
-                 const csffci_link_t* link_b, const double* ci, double* sigma, int flags, int eta,
-                 void* work, size_t work_bytes, cudaStream_t stream) {
+}  // extern "C"
+
+namespace csffci {
+// csffci_sigma with an explicit kernel choice: variant -1 is the default
+// for one problem (sigma_rr_single_variant), -2 the shared-memory-h2e
+// kernel (as CSFFCI_SIGMA_REFERENCE_KERNEL), anything else a variant of the
+// register-resident family (sigma_rr.cu)
+static int sigma_exec(int norb, int neleca, int nelecb, const double* h2e, const csffci_link_t* link_a,
+                      const csffci_link_t* link_b, const double* ci, double* sigma, int flags, int eta,
+                      void* work, size_t work_bytes, int variant, cudaStream_t stream) {
   CSF_REQUIRE(norb >= 1 && norb <= 22, "sigma: norb=%d outside [1,22]", norb);
   CSF_REQUIRE(neleca >= 0 && nelecb >= 0 && neleca <= norb && nelecb <= norb,
               "sigma: bad nelec (%d,%d)", neleca, nelecb);
@@ -328,8 +337,9 @@ int csffci_sigma(int norb, int neleca, int nelecb, const double* h2e, const csff
   if (sym || !accumulate) CSF_CUDA(cudaMemsetAsync(target, 0, ndet * sizeof(double), stream));
   if (ndet == 0) return CSFFCI_OK;
 
-  if (sigma_rr_supported(norb) && !(flags & CSFFCI_SIGMA_REFERENCE_KERNEL)) {
-    int st = sigma_rr_run(norb, neleca, nelecb, h2e, link_a, link_b, ci, target, sym, (double)eta, stream);
+  if (sigma_rr_supported(norb) && !(flags & CSFFCI_SIGMA_REFERENCE_KERNEL) && variant != -2) {
+    int st = sigma_rr_run(norb, neleca, nelecb, h2e, link_a, link_b, ci, target, sym, (double)eta, stream,
+                          variant);
     if (st) return st;
     if (sym) {
       dim3 blk(32, 8);
@@ -394,5 +404,92 @@ int csffci_sigma(int norb, int neleca, int nelecb, const double* h2e, const csff
   }
   return CSFFCI_OK;
 }
+}  // namespace csffci
+
+// ---- sigma plan: the per-problem state of csffci_sigma bound once ------
+struct csffci_sigma_plan {
+  int norb, neleca, nelecb, flags, variant;
+  const double* h2e;
+  const csffci_link_t* link_a;
+  const csffci_link_t* link_b;
+  size_t work_bytes;
+  void* work;
+};
+
+extern "C" {
+
+int csffci_sigma(int norb, int neleca, int nelecb, const double* h2e, const csffci_link_t* link_a,
+                 const csffci_link_t* link_b, const double* ci, double* sigma, int flags, int eta,
+                 void* work, size_t work_bytes, cudaStream_t stream) {
+  return sigma_exec(norb, neleca, nelecb, h2e, link_a, link_b, ci, sigma, flags, eta, work, work_bytes, -1,
+                    stream);
+}
+
+int csffci_sigma_plan_create(int norb, int neleca, int nelecb, const double* h2e, const csffci_link_t* link_a,
+                             const csffci_link_t* link_b, int flags, csffci_sigma_plan_t** plan,
+                             size_t* work_bytes) {
+  CSF_REQUIRE(plan != nullptr, "sigma_plan_create: plan is NULL");
+  *plan = nullptr;
+  CSF_REQUIRE(norb >= 1 && norb <= 22, "sigma_plan_create: norb=%d outside [1,22]", norb);
+  CSF_REQUIRE(neleca >= 0 && nelecb >= 0 && neleca <= norb && nelecb <= norb,
+              "sigma_plan_create: bad nelec (%d,%d)", neleca, nelecb);
+  CSF_REQUIRE(h2e != nullptr && link_a != nullptr && link_b != nullptr,
+              "sigma_plan_create: h2e and the link tables are required");
+  CSF_REQUIRE((flags & ~(CSFFCI_SIGMA_SPIN_SYMMETRIC | CSFFCI_SIGMA_REFERENCE_KERNEL)) == 0,
+              "sigma_plan_create: flags may hold SPIN_SYMMETRIC and REFERENCE_KERNEL only");
+  CSF_REQUIRE(!(flags & CSFFCI_SIGMA_SPIN_SYMMETRIC) || neleca == nelecb,
+              "sigma_plan_create: the spin-symmetric mode needs neleca == nelecb");
+  csffci_sigma_plan_t* p = new (std::nothrow) csffci_sigma_plan_t;
+  if (!p) {
+    set_error("sigma_plan_create: out of host memory");
+    return CSFFCI_ERR_MEMORY;
+  }
+  p->norb = norb;
+  p->neleca = neleca;
+  p->nelecb = nelecb;
+  p->flags = flags;
+  p->h2e = h2e;
+  p->link_a = link_a;
+  p->link_b = link_b;
+  p->variant = (flags & CSFFCI_SIGMA_REFERENCE_KERNEL) || !sigma_rr_supported(norb)
+                   ? -2
+                   : sigma_rr_single_variant(norb);
+  if (p->variant < 0 && p->variant != -2) p->variant = rr_default_variant(norb);
+  p->work_bytes = csffci_sigma_workspace(norb, neleca, nelecb, flags);
+  p->work = nullptr;
+  if (work_bytes) *work_bytes = p->work_bytes;
+  *plan = p;
+  return CSFFCI_OK;
+}
+
+int csffci_sigma_plan_bind(csffci_sigma_plan_t* plan, void* work, size_t work_bytes) {
+  CSF_REQUIRE(plan != nullptr, "sigma_plan_bind: plan is NULL");
+  if (plan->work_bytes && (work == nullptr || work_bytes < plan->work_bytes)) {
+    set_error("sigma_plan_bind: workspace of %zu bytes < %zu required", work_bytes, plan->work_bytes);
+    return CSFFCI_ERR_MEMORY;
+  }
+  plan->work = work;
+  return CSFFCI_OK;
+}
+
+int csffci_sigma_plan_execute(const csffci_sigma_plan_t* plan, const double* ci, double* sigma, int eta,
+                              int flags, cudaStream_t stream) {
+  CSF_REQUIRE(plan != nullptr, "sigma_plan_execute: plan is NULL");
+  CSF_REQUIRE((flags & ~(CSFFCI_SIGMA_ACCUMULATE | CSFFCI_SIGMA_SPIN_SYMMETRIC)) == 0,
+              "sigma_plan_execute: flags may hold ACCUMULATE and SPIN_SYMMETRIC only");
+  CSF_REQUIRE(!(flags & CSFFCI_SIGMA_SPIN_SYMMETRIC) || (plan->flags & CSFFCI_SIGMA_SPIN_SYMMETRIC),
+              "sigma_plan_execute: the plan was created without the spin-symmetric mode");
+  CSF_REQUIRE(!plan->work_bytes || plan->work != nullptr, "sigma_plan_execute: the plan has no workspace bound");
+  return sigma_exec(plan->norb, plan->neleca, plan->nelecb, plan->h2e, plan->link_a, plan->link_b, ci, sigma,
+                    flags | (plan->flags & CSFFCI_SIGMA_REFERENCE_KERNEL), eta, plan->work, plan->work_bytes,
+                    plan->variant, stream);
+}
+
+int csffci_sigma_plan_variant(const csffci_sigma_plan_t* plan) {
+  CSF_REQUIRE(plan != nullptr, "sigma_plan_variant: plan is NULL");
+  return plan->variant;
+}
+
+void csffci_sigma_plan_destroy(csffci_sigma_plan_t* plan) { delete plan; }
 
 }  // extern "C"

@@ -53,11 +53,12 @@ bool rr_variant_valid(int norb, int v) { return v >= 0 && v < RR_NVARIANT && !(v
 
 // one problem: the warp-specialised kernel from 14 orbitals (CSFFCI_SIGMA_VARIANT
 // may name any variant); -1 leaves the choice to rr_default_variant
-static int rr_single_variant(int norb) {
+int sigma_rr_single_variant(int norb) {
   const char* env = getenv("CSFFCI_SIGMA_VARIANT");
   if (env) {
     const int v = atoi(env);
     if (v == RR_VARIANT_WS && sigma_ws_supported(norb)) return RR_VARIANT_WS;
+    if (v == RR_VARIANT_WSR && sigma_wsr_supported(norb)) return RR_VARIANT_WSR;
     if (rr_variant_valid(norb, v)) return v;
   }
   // measured on B200 (singlet, one problem): 14 orbitals 7.61 -> 6.31 ms,
@@ -105,7 +106,7 @@ int sigma_rr_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev,
                     int max_nla, int max_nlb, cudaStream_t stream, int variant) {
   const int npair = norb * (norb + 1) / 2;
   const int ks = (npair + 3) / 4;
-  if (variant < 0 && !jobs_dev) variant = rr_single_variant(norb);
+  if (variant < 0 && !jobs_dev) variant = sigma_rr_single_variant(norb);
   if (variant < 0) variant = rr_default_variant(norb);
   if (variant == RR_VARIANT_WS) {
     if (jobs_dev) {
@@ -113,6 +114,13 @@ int sigma_rr_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev,
       return CSFFCI_ERR_INVALID;
     }
     return sigma_ws_launch(norb, job0, total_units, max_nb, max_nla, max_nlb, stream);
+  }
+  if (variant == RR_VARIANT_WSR) {
+    if (jobs_dev) {
+      set_error("sigma: the register-split variant takes one problem, not a job table");
+      return CSFFCI_ERR_INVALID;
+    }
+    return sigma_wsr_launch(norb, job0, total_units, max_nb, max_nla, max_nlb, stream);
   }
   if (!rr_variant_valid(norb, variant)) {
     set_error("sigma: tile variant %d is not available for norb=%d", variant, norb);
@@ -159,7 +167,7 @@ switch (variant) {
 
 int sigma_rr_run(int norb, int neleca, int nelecb, const double* h2e, const csffci_link_t* la,
                  const csffci_link_t* lb, const double* ci, double* out, bool sym, double eta,
-                 cudaStream_t stream) {
+                 cudaStream_t stream, int variant) {
   CSF_REQUIRE(rr_aligned8(la) && rr_aligned8(lb) && rr_aligned8(ci) && rr_aligned8(out),
               "sigma: link tables and vectors must be 8-byte aligned");
   csffci_sigma_job_t J;
@@ -177,7 +185,7 @@ int sigma_rr_run(int norb, int neleca, int nelecb, const double* h2e, const csff
   long long total, maxnb;
   int mla, mlb;
   rr_prepare(norb, 1, &J, &total, &maxnb, &mla, &mlb);
-  return sigma_rr_launch(norb, 1, nullptr, J, total, maxnb, mla, mlb, stream, -1);
+  return sigma_rr_launch(norb, 1, nullptr, J, total, maxnb, mla, mlb, stream, variant);
 }
 
 // ---- batch: zero the outputs, run the jobs, form sigma = S + eta S^T -----

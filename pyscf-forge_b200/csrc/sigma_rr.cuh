@@ -5,7 +5,14 @@
 
 namespace csffci {
 bool sigma_rr_supported(int norb);
+// variant: tile variant of the register-resident family (0..3), 4 or 5 for
+// the warp-specialised kernels, -1 for the default of one problem
 int sigma_rr_run(int norb, int neleca, int nelecb, const double* h2e, const csffci_link_t* la,
                  const csffci_link_t* lb, const double* ci, double* out, bool sym, double eta,
-                 cudaStream_t stream);
+                 cudaStream_t stream, int variant = -1);
+// the kernel variant one problem of norb orbitals runs by default
+// (CSFFCI_SIGMA_VARIANT overrides it)
+int sigma_rr_single_variant(int norb);
+// the register-resident tile variant of norb orbitals (0..3)
+int rr_default_variant(int norb);
 }  // namespace csffci

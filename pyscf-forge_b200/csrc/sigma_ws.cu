@@ -31,26 +31,9 @@
 // scheduler: the register budget of k_sigma_rr, which the A fragments need.
 #include <stdlib.h>
 
-#include "sigma_rr_kernel.cuh"
+#include "sigma_ws.cuh"
 
 namespace csffci {
-
-__device__ __forceinline__ void ws_bar_sync(int id, int nthreads) {
-  asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(nthreads) : "memory");
-}
-
-__device__ __forceinline__ void ws_bar_arrive(int id, int nthreads) {
-  asm volatile("bar.arrive %0, %1;\n" ::"r"(id), "r"(nthreads) : "memory");
-}
-
-__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-
-// m8n8k4 FP64 MMA accumulating into (c0, c1): A row g col t, B row t col g
-__device__ __forceinline__ void ws_dmma(double& c0, double& c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(c0), "+d"(c1)
-               : "d"(a), "d"(b));
-}
 
 // MMA warps: one per m-tile of 8 rows, the last m-tiles split over two warps
 // (one n-tile each) when MT mod 4 is 1 or 2; movers fill the CTA to a
@@ -69,81 +52,7 @@ struct WSLayout {
   static constexpr int NMOV = NTOT - NWM;
 };
 
-constexpr int WS_NB = 16;     // columns per tile
-constexpr int WS_STAGES = 3;  // ring of D/V and link buffers
 constexpr int WS_RU = 4;      // links a mover thread handles together (loads in flight)
-
-// The shared state of the row Ja a CTA works on.
-struct WSShared {
-  double* Dbuf;
-  csffci_link_t* Lbuf;
-  double* crow;
-  RRAlpha* al;
-  int* zl;
-  unsigned* pneg;
-  int* zf;
-  RRRow* srow;
-  long long* apoff;  // per pair row: Ka*Nb of its alpha link in row Ja, -1 without one
-};
-
-// Row setup shared by both roles (every thread of the CTA calls it with the
-// same arguments, and it synchronises the CTA on barrier 9): the alpha links
-// of row Ja, the rows without one, the sign masks of this row (in half par
-// of pneg) and the copy of c row Ja.  Returns false (for every thread) when
-// the spin-symmetric unit has no second row.
-template <int NTH, int NB>
-__device__ __forceinline__ bool ws_row_setup(const RRArgs& g, const WSShared& S, long long lu, int w, int par,
-                                             int tid, int warp, int lane) {
-  const csffci_sigma_job_t& sjob = g.job0;
-  const long long Nb = sjob.Nb;
-  const int nla = sjob.nla, npair = g.npair, ds = g.ds;
-  long long ja = lu;
-  if (sjob.sym && w == 1) {
-    ja = sjob.Na - 1 - lu;
-    if (ja <= lu) return false;
-  }
-  unsigned* const pcur = S.pneg + par * npair;
-  ws_bar_sync(9, NTH);  // the previous row is fully consumed
-  if (tid == 0) {
-    S.srow->ja = ja;
-    S.srow->jend = sjob.sym ? ja + 1 : Nb;
-    S.srow->nchunk = (int)((S.srow->jend + NB - 1) / NB);
-    S.srow->pc = par * npair;
-  }
-  for (int r = tid; r < npair; r += NTH) {
-    pcur[r] = 0u;
-    S.zf[r] = 1;
-    S.apoff[r] = -1;
-  }
-  ws_bar_sync(9, NTH);
-  for (int l = tid; l < nla; l += NTH) {
-    const uint2 e = rr_link(&sjob.link_a[ja * nla + l]);
-    const int pr = rr_lpair(e);
-    RRAlpha a;
-    a.off = (long long)e.x * Nb;
-    a.drow = pr * ds;
-    a.neg = rr_lneg(e);
-    S.al[l] = a;
-    pcur[pr] = a.neg;
-    S.zf[pr] = 0;
-    S.apoff[pr] = a.off;
-  }
-  for (long long i = tid; i < Nb; i += NTH) cp_async8(&S.crow[i], &sjob.ci[ja * Nb + i]);
-  cp_async_commit();
-  ws_bar_sync(9, NTH);
-  if (warp == 0) {
-    int n = 0;
-    for (int base = 0; base < npair; base += 32) {
-      const int r = base + lane;
-      const bool z = r < npair && S.zf[r];
-      const unsigned bal = __ballot_sync(0xffffffffu, z);
-      if (z) S.zl[n + __popc(bal & ((1u << lane) - 1u))] = r * ds;
-      n += __popc(bal);
-    }
-    if (lane == 0) S.srow->nzero = n;
-  }
-  return true;
-}
 
 template <int KS, int MT>
 __global__ void __launch_bounds__(WSLayout<MT>::NTOT * 32, 1) k_sigma_ws(RRArgs g) {
@@ -151,8 +60,6 @@ __global__ void __launch_bounds__(WSLayout<MT>::NTOT * 32, 1) k_sigma_ws(RRArgs 
   constexpr int NB = WS_NB;
   constexpr int NTH = L::NTOT * 32;
   constexpr int NWM = L::NWM, NMOV = L::NMOV;
-  constexpr int MTH = NMOV * 32;   // mover threads
-  constexpr int MPASS = MTH / NB;  // link rows per mover pass (threads over the NB columns)
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ RRRow srow;
   WSShared S;
@@ -168,9 +75,9 @@ __global__ void __launch_bounds__(WSLayout<MT>::NTOT * 32, 1) k_sigma_ws(RRArgs 
   const csffci_sigma_job_t& sjob = g.job0;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int ds = g.ds, LS = g.ls, npair = g.npair;
+  const int ds = g.ds, npair = g.npair;
   const int ndr = g.nd_rows;
-  const size_t dsz = (size_t)ndr * ds, lsz = (size_t)NB * LS;
+  const size_t dsz = (size_t)ndr * ds;
   for (int i = tid; i < (ndr - npair) * ds; i += NTH)
     for (int s = 0; s < WS_STAGES; ++s) S.Dbuf[s * dsz + npair * ds + i] = 0.0;
 
@@ -261,119 +168,7 @@ __global__ void __launch_bounds__(WSLayout<MT>::NTOT * 32, 1) k_sigma_ws(RRArgs 
       }
     }
   } else {
-    // ---- movers: copies, beta gather, scatters ----
-    const int mtid = tid - NWM * 32;
-    const int mwarp = warp - NWM;
-    const int jl = mtid % NB, ml = mtid / NB;
-    int par = 0;
-    for (long long u = blockIdx.x; u < g.total_units; u += gridDim.x) {
-      const long long lu = u - sjob.unit_begin;
-      for (int w = 0; w < (sjob.sym ? 2 : 1); ++w) {
-        if (!ws_row_setup<NTH, NB>(g, S, lu, w, par, tid, warp, lane)) break;
-        par ^= 1;
-        cp_async_wait_all();
-        ws_bar_sync(9, NTH);
-        const int nch = srow.nchunk;
-        const long long jend = srow.jend, ja = srow.ja, Nb = sjob.Nb;
-        const int nla = sjob.nla, nlb = sjob.nlb, nz = srow.nzero;
-        const unsigned* pc = S.pneg + srow.pc;
-        const bool SYM = sjob.sym != 0;
-        double* const out = SYM ? sjob.scratch : sjob.sigma;
-        for (int c = 0; c <= nch + 1; ++c) {
-          // every mover has finished step c-1 (its scatter read the stage
-          // that the copies below refill)
-          ws_bar_sync(7, MTH);
-          if (c < nch) {
-            // copies of tile c into stage c % 3 (its last tile, c-3, was
-            // scattered at step c-1): alpha rows of c, beta links, zero rows
-            const int s = c % WS_STAGES;
-            double* Dd = S.Dbuf + s * dsz;
-            csffci_link_t* Ld = S.Lbuf + s * lsz;
-            const long long j1 = (long long)c * NB;
-            const int nc = (int)min((long long)NB, jend - j1);
-            if (jl < nc) {
-              const double* src = sjob.ci + j1 + jl;
-              for (int l0 = ml; l0 < nla; l0 += WS_RU * MPASS) {
-                RRAlpha a[WS_RU];
-#pragma unroll
-                for (int k = 0; k < WS_RU; ++k) a[k] = S.al[min(l0 + k * MPASS, nla - 1)];
-#pragma unroll
-                for (int k = 0; k < WS_RU; ++k)
-                  if (l0 + k * MPASS < nla) cp_async8(&Dd[a[k].drow + jl], src + a[k].off);
-              }
-            }
-            const csffci_link_t* lsrc = sjob.link_b + j1 * nlb;
-            for (int jb = mwarp; jb < nc; jb += NMOV)
-              for (int m = lane; m < nlb; m += 32) cp_async8(&Ld[jb * LS + m], &lsrc[(long long)jb * nlb + m]);
-            cp_async_commit();
-            const int zr = lane / (NB / 2), zc = 2 * (lane % (NB / 2));
-            for (int i = mwarp * 4 + zr; i < nz; i += NMOV * 4)
-              *reinterpret_cast<double2*>(&Dd[S.zl[i] + zc]) = make_double2(0.0, 0.0);
-          }
-          if (c >= 1 && c - 1 < nch) {
-            // gather of tile c-1: its copies have landed (the newest group,
-            // tile c, may still be in flight)
-            if (c < nch) cp_async_wait_one();
-            else cp_async_wait_all();
-            ws_bar_sync(7, MTH);
-            const int s = (c - 1) % WS_STAGES;
-            double* D = S.Dbuf + s * dsz;
-            const csffci_link_t* Lt = S.Lbuf + s * lsz;
-            const int ncol = (int)min((long long)NB, jend - (long long)(c - 1) * NB);
-            if (jl < ncol)
-              for (int m0 = ml; m0 < nlb; m0 += WS_RU * MPASS) {
-                // WS_RU links per pass, every load of the pass issued before
-                // the dependent ones (distinct links of a column have
-                // distinct pairs, so the read-modify-writes do not overlap)
-                uint2 e[WS_RU];
-                double v[WS_RU], d[WS_RU];
-                unsigned f[WS_RU];
-#pragma unroll
-                for (int k = 0; k < WS_RU; ++k) {
-                  const int m = m0 + k * MPASS;
-                  e[k] = m < nlb ? rr_link(&Lt[jl * LS + m]) : make_uint2(0u, 0u);
-                }
-#pragma unroll
-                for (int k = 0; k < WS_RU; ++k) {
-                  v[k] = S.crow[e[k].x];
-                  f[k] = rr_lneg(e[k]) ^ pc[rr_lpair(e[k])];
-                  d[k] = D[rr_lpair(e[k]) * ds + jl];
-                }
-#pragma unroll
-                for (int k = 0; k < WS_RU; ++k)
-                  if (m0 + k * MPASS < nlb) D[rr_lpair(e[k]) * ds + jl] = d[k] + rr_flip(v[k], f[k]);
-              }
-            ws_bar_arrive(1 + s, NTH);  // D of tile c-1 is gathered
-          }
-          if (c >= 2) {
-            // scatter of tile c-2
-            const int s = (c - 2) % WS_STAGES;
-            ws_bar_sync(4 + s, NTH);  // V of tile c-2 is written
-            const double* D = S.Dbuf + s * dsz;
-            const csffci_link_t* Lt = S.Lbuf + s * lsz;
-            const long long j0 = (long long)(c - 2) * NB;
-            const int ncol = (int)min((long long)NB, jend - j0);
-            if (jl < ncol) {
-              double* const orow = out + ja * Nb;
-              for (int m0 = ml; m0 < nlb; m0 += WS_RU * MPASS) {
-                uint2 e[WS_RU];
-                double v[WS_RU];
-#pragma unroll
-                for (int k = 0; k < WS_RU; ++k) {
-                  const int m = m0 + k * MPASS;
-                  e[k] = m < nlb ? rr_link(&Lt[jl * LS + m]) : make_uint2(0u, 0u);
-                }
-#pragma unroll
-                for (int k = 0; k < WS_RU; ++k) v[k] = D[rr_lpair(e[k]) * ds + jl];
-#pragma unroll
-                for (int k = 0; k < WS_RU; ++k)
-                  if (m0 + k * MPASS < nlb) atomicAdd(&orow[e[k].x], rr_flip(v[k], rr_lneg(e[k])));
-              }
-            }
-          }
-        }
-      }
-    }
+    ws_mover_role<NTH, NMOV, WS_RU>(g, S, tid, warp, lane, tid - NWM * 32, warp - NWM);
   }
 }
 
@@ -400,24 +195,13 @@ static int launch_ws(RRArgs& g, size_t smem, cudaStream_t stream) {
   return check_launch("sigma (warp-specialised)");
 }
 
-int sigma_ws_launch(int norb, const csffci_sigma_job_t& job0, long long total_units, long long max_nb,
-                    int max_nla, int max_nlb, cudaStream_t stream) {
-  if (!sigma_ws_supported(norb)) {
-    set_error("sigma: the warp-specialised variant covers norb 13..16, not %d", norb);
-    return CSFFCI_ERR_INVALID;
-  }
-  const int npair = norb * (norb + 1) / 2;
+size_t ws_layout(RRArgs& g, int npair, int rows_multiple, long long max_nb, int max_nla, int max_nlb,
+                 size_t extra_bytes, unsigned* extra_off) {
   const int ks = (npair + 3) / 4;
-  RRArgs g;
-  memset(&g, 0, sizeof(g));
-  g.jobs = nullptr;
-  g.job0 = job0;
-  g.njobs = 1;
-  g.total_units = total_units;
   g.npair = npair;
   g.ds = WS_NB + 4;  // = 4 (mod 16): conflict-free B-fragment loads
   g.ls = max_nlb | 1;
-  const int rows_w = ((npair + 7) / 8) * 8;
+  const int rows_w = ((npair + rows_multiple - 1) / rows_multiple) * rows_multiple;
   g.nd_rows = 4 * ks > rows_w ? 4 * ks : rows_w;
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -433,9 +217,29 @@ int sigma_ws_launch(int norb, const csffci_sigma_job_t& job0, long long total_un
   g.off_pn = take((size_t)2 * npair * sizeof(unsigned));
   g.off_zf = take((size_t)npair * sizeof(int));
   g.off_ap = take((size_t)npair * sizeof(long long));  // per-pair alpha offsets
-  const size_t smem = off;
-  if (smem > 227 * 1024 - 256) {
-    set_error("sigma: warp-specialised tiles of %zu bytes exceed shared memory", smem);
+  if (extra_bytes) {
+    const unsigned o = take(extra_bytes);
+    if (extra_off) *extra_off = o;
+  }
+  return off > 227 * 1024 - 256 ? 0 : off;
+}
+
+int sigma_ws_launch(int norb, const csffci_sigma_job_t& job0, long long total_units, long long max_nb,
+                    int max_nla, int max_nlb, cudaStream_t stream) {
+  if (!sigma_ws_supported(norb)) {
+    set_error("sigma: the warp-specialised variant covers norb 13..16, not %d", norb);
+    return CSFFCI_ERR_INVALID;
+  }
+  const int npair = norb * (norb + 1) / 2;
+  RRArgs g;
+  memset(&g, 0, sizeof(g));
+  g.jobs = nullptr;
+  g.job0 = job0;
+  g.njobs = 1;
+  g.total_units = total_units;
+  const size_t smem = ws_layout(g, npair, 8, max_nb, max_nla, max_nlb, 0, nullptr);
+  if (smem == 0) {
+    set_error("sigma: warp-specialised tiles exceed shared memory (norb %d)", norb);
     return CSFFCI_ERR_INVALID;
   }
   switch (norb) {

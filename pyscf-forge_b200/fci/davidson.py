@@ -87,10 +87,11 @@ class DiagPrecond:
 
 
 def davidson(aop, x0, precond, tol=1e-10, max_cycle=100, max_space=12, lindep=1e-14, nroots=1,
-             follow_state=True, tol_residual=None, verbose=0, log=None):
+             follow_state=True, tol_residual=None, verbose=0, log=None, stats=None):
     """aop(X) maps a device (k, n) block to (k, n).  x0: device (m, n) or a
     list of device vectors.  Returns (converged list, energies numpy,
-    device (nroots, n) eigenvectors)."""
+    device (nroots, n) eigenvectors); stats (a dict, optional) receives the
+    number of iterations as stats["niter"]."""
     if callable(x0):
         x0 = x0()
     if isinstance(x0, (list, tuple)):
@@ -115,6 +116,8 @@ def davidson(aop, x0, precond, tol=1e-10, max_cycle=100, max_space=12, lindep=1e
     nrm = np.sqrt(np.maximum(np.diag(gram(new, new).cpu().numpy()), 1e-300))
     new = new / torch.as_tensor(nrm, device=dev)[:, None]
     for icyc in range(max_cycle):
+        if stats is not None:
+            stats["niter"] = icyc + 1
         # orthonormalise the new block against V and among itself
         added = []
         for i in range(new.shape[0]):

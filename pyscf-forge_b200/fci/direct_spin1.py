@@ -8,6 +8,7 @@ and return torch CUDA tensors; the PySCF-style functions accept numpy or
 torch and answer in the caller's type.
 """
 import ctypes
+import os
 from math import comb
 
 import numpy as np
@@ -88,24 +89,98 @@ def dev_make_hdiag(h1a, h1b, eri4, norb, nelec):
     return out
 
 
+class SigmaPlan:
+    """csffci_sigma_plan for one (norb, nelec, h2e): link tables, kernel
+    choice and workspace bound once, then executed per vector (the model of
+    the reference's fci_contract_gas_plan, pyscf/lib/mcscf/fci_gas.h:244-253).
+    Holds references to h2e and the link tables, whose device memory the
+    plan borrows; the kernel is fixed at creation (CSFFCI_SIGMA_VARIANT is
+    read then)."""
+
+    def __init__(self, h2e, norb, nelec, spin_symmetric=False):
+        require_cuda()
+        na, nb = nelec
+        self.norb, self.nelec = int(norb), (int(na), int(nb))
+        self.h2e = h2e.contiguous()
+        self.la = dev_link_table(norb, na)
+        self.lb = dev_link_table(norb, nb)
+        self.sym = bool(spin_symmetric) and na == nb
+        flags = _capi.SIGMA_SPIN_SYMMETRIC if self.sym else 0
+        h = ctypes.c_void_p()
+        nbytes = ctypes.c_size_t()
+        _capi.call("csffci_sigma_plan_create", self.norb, na, nb, ptr(self.h2e), ptr(self.la), ptr(self.lb),
+                   flags, ctypes.byref(h), ctypes.byref(nbytes))
+        self._h = h
+        self.work_bytes = int(nbytes.value)
+        self._bound = None
+        self.variant = _capi.query("csffci_sigma_plan_variant", h)
+
+    def __call__(self, ci, out, eta=None, accumulate=False):
+        flags = _capi.SIGMA_ACCUMULATE if accumulate else 0
+        if eta is not None:
+            if not self.sym:
+                raise ValueError("the plan was created without the spin-symmetric mode")
+            flags |= _capi.SIGMA_SPIN_SYMMETRIC
+        if self.work_bytes:
+            # the spin-symmetric scratch is the shared stream-ordered sigma
+            # workspace (one per device, not one per plan); rebind when it
+            # was reallocated
+            ws = workspace("sigma", self.work_bytes)
+            if ws.data_ptr() != self._bound:
+                _capi.call("csffci_sigma_plan_bind", self._h, ptr(ws), ws.numel())
+                self._bound = ws.data_ptr()
+        _capi.call("csffci_sigma_plan_execute", self._h, ptr(ci), ptr(out), int(eta or 1), flags, stream())
+        return out
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h is not None and _capi._LIB is not None:
+            _capi._LIB.csffci_sigma_plan_destroy(h)
+
+
+_PLAN_CACHE = {}
+_PLAN_CACHE_SIZE = 8
+
+
+def sigma_plan(h2e, norb, nelec):
+    """The cached SigmaPlan of (device, norb, nelec, h2e tensor); the cache
+    keeps the h2e tensor alive, so its address names it, and holds at most
+    _PLAN_CACHE_SIZE plans (least recently used dropped first)."""
+    key = (torch.cuda.current_device(), int(norb), int(nelec[0]), int(nelec[1]), h2e.data_ptr(),
+           tuple(h2e.shape))
+    plan = _PLAN_CACHE.pop(key, None)
+    if plan is None or plan.h2e.data_ptr() != h2e.data_ptr():
+        plan = SigmaPlan(h2e, norb, nelec, spin_symmetric=nelec[0] == nelec[1])
+    _PLAN_CACHE[key] = plan
+    while len(_PLAN_CACHE) > _PLAN_CACHE_SIZE:
+        _PLAN_CACHE.pop(next(iter(_PLAN_CACHE)))
+    return plan
+
+
 def dev_contract_2e(h2e, ci, norb, nelec, eta=None, out=None, accumulate=False):
     """sigma = sum h2e[pq,rs] E_pq E_rs ci on the device.  eta (+1/-1) asserts
-    ci = eta ci^T (na == nb) and selects the row-local kernel."""
+    ci = eta ci^T (na == nb) and selects the row-local kernel.  Runs through
+    the cached sigma plan of (norb, nelec, h2e)."""
     na, nb = nelec
-    la = dev_link_table(norb, na)
-    lb = dev_link_table(norb, nb)
     ci = ci.contiguous()
     if out is None:
         out = torch.empty_like(ci)
         accumulate = False
-    flags = _capi.SIGMA_ACCUMULATE if accumulate else 0
-    if eta is not None:
-        flags |= _capi.SIGMA_SPIN_SYMMETRIC
-    nbytes = _capi.query("csffci_sigma_workspace", norb, na, nb, flags)
-    ws = workspace("sigma", nbytes) if nbytes else None
-    _capi.call("csffci_sigma", norb, na, nb, ptr(h2e), ptr(la), ptr(lb), ptr(ci), ptr(out), flags,
-               int(eta or 1), ptr(ws), nbytes, stream())
-    return out
+    h2e = h2e if h2e.is_contiguous() else h2e.contiguous()
+    if os.environ.get("CSFFCI_SIGMA_VARIANT") is not None:
+        # a kernel named for this call (tests, profiling): an unplanned call
+        # reads the variable on every launch
+        la = dev_link_table(norb, na)
+        lb = dev_link_table(norb, nb)
+        flags = _capi.SIGMA_ACCUMULATE if accumulate else 0
+        if eta is not None:
+            flags |= _capi.SIGMA_SPIN_SYMMETRIC
+        nbytes = _capi.query("csffci_sigma_workspace", norb, na, nb, flags)
+        ws = workspace("sigma", nbytes) if nbytes else None
+        _capi.call("csffci_sigma", norb, na, nb, ptr(h2e), ptr(la), ptr(lb), ptr(ci), ptr(out), flags,
+                   int(eta or 1), ptr(ws), nbytes, stream())
+        return out
+    return sigma_plan(h2e, norb, (na, nb))(ci, out, eta=eta, accumulate=accumulate)
 
 
 def dev_spin_parity(ci, n, rtol=1e-12):

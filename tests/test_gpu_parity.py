@@ -98,6 +98,25 @@ def test_spin_evecs_bit_exact():
                 assert np.array_equal(u, ref), (nspin, na, nb, smult)
 
 
+@needs_ref
+@pytest.mark.parametrize("nspin", [13, 14, 15, 16])
+def test_spin_evecs_bit_exact_large(nspin):
+    """The large spin-coupling blocks (up to 16 unpaired electrons, the
+    12870 x 1430 singlet block every CAS(16,16) transform multiplies by)
+    against FCICSFmakecsf (csfstring.c:86-141), bit for bit, at the smallest
+    |2MS| and every spin multiplicity."""
+    _, _, C = _mods()
+    na = (nspin + 1) // 2
+    nb = nspin - na
+    det = R.addrs2str(nspin, na, np.arange(R.num_strings(nspin, na)))
+    for smult in range(abs(na - nb) + 1, nspin + 2, 2):
+        u = C.get_spin_evecs(nspin, na, nb, smult).cpu().numpy()
+        coup = R.gen_addrs2str(nspin, smult, np.arange(u.shape[1]))
+        ref = gasref.makecsf(det, coup, nspin, smult - 1, na - nb)
+        assert np.array_equal(u, ref), (nspin, na, nb, smult)
+        del u, ref
+
+
 def test_spin_evecs_fixture(golden_case):
     _, _, C = _mods()
     n, na, nb, sm = _case(golden_case)
@@ -407,12 +426,14 @@ def test_solver_contract_2e_out_buffers():
 
 @needs_ref
 @pytest.mark.parametrize("norb,nelec,rank", [(14, (3, 3), 10), (14, (3, 2), 10), (15, (4, 3), 10),
-                                             (16, (2, 2), 8), (13, (3, 3), 8)])
+                                             (16, (2, 2), 8), (13, (3, 3), 8), (16, (3, 3), 8),
+                                             (16, (3, 2), 8)])
 def test_warp_specialised_sigma(norb, nelec, rank, monkeypatch):
-    """The warp-specialised sigma kernel (tile variant 4, the single-problem
-    default from 14 orbitals): against the reference C (1e-10) and against
-    the phase-serial kernel (1e-12), in the general and, for na == nb, the
-    spin-symmetric mode."""
+    """The warp-specialised sigma kernels (tile variant 4 from 13 orbitals,
+    variant 5 -- registers re-split between the roles -- at 16): against the
+    reference C (1e-10) and against the phase-serial kernel (1e-12), in the
+    general mode and, for na == nb, the spin-symmetric mode with a symmetric
+    (eta = +1) and an antisymmetric (eta = -1) vector."""
     import torch
     _, D, _ = _mods()
     from math import comb
@@ -421,18 +442,73 @@ def test_warp_specialised_sigma(norb, nelec, rank, monkeypatch):
     h2e = torch.as_tensor(h2e_np, device="cuda")
     na, nb = comb(norb, nelec[0]), comb(norb, nelec[1])
     rng = np.random.default_rng(12)
-    c = rng.normal(size=(na, nb))
+    c0 = rng.normal(size=(na, nb))
+    cases = [(c0, (None,))]
     if na == nb:
-        c = c + c.T
-    c /= np.linalg.norm(c)
-    ref = gasref.contract_2e(h2e_np, c, norb, nelec).ravel()
-    cd = torch.as_tensor(c.ravel(), device="cuda")
-    etas = (None, 1) if na == nb else (None,)
-    for eta in etas:
-        monkeypatch.setenv("CSFFCI_SIGMA_VARIANT", "4")
-        ws = D.dev_contract_2e(h2e, cd, norb, nelec, eta=eta).cpu().numpy()
-        monkeypatch.setenv("CSFFCI_SIGMA_VARIANT", "1")
-        rr = D.dev_contract_2e(h2e, cd, norb, nelec, eta=eta).cpu().numpy()
-        np.testing.assert_allclose(ws, ref, atol=1e-10)
-        np.testing.assert_allclose(ws, rr, atol=1e-12)
+        cases = [(c0 + c0.T, (None, 1)), (c0 - c0.T, (-1,))]
+    variants = (4, 5) if norb == 16 else (4,)
+    for c, etas in cases:
+        c = c / np.linalg.norm(c)
+        ref = gasref.contract_2e(h2e_np, c, norb, nelec).ravel()
+        cd = torch.as_tensor(c.ravel(), device="cuda")
+        for eta in etas:
+            monkeypatch.setenv("CSFFCI_SIGMA_VARIANT", "1")
+            rr = D.dev_contract_2e(h2e, cd, norb, nelec, eta=eta).cpu().numpy()
+            for v in variants:
+                monkeypatch.setenv("CSFFCI_SIGMA_VARIANT", str(v))
+                ws = D.dev_contract_2e(h2e, cd, norb, nelec, eta=eta).cpu().numpy()
+                np.testing.assert_allclose(ws, ref, atol=1e-10)
+                np.testing.assert_allclose(ws, rr, atol=1e-12)
     monkeypatch.delenv("CSFFCI_SIGMA_VARIANT")
+
+
+@pytest.mark.parametrize("norb,nelec,smult", [(8, (4, 4), 1), (12, (6, 6), 3), (11, (6, 5), 2),
+                                              (16, (3, 3), 1)])
+def test_sigma_plan_c_abi(norb, nelec, smult):
+    """csffci_sigma_plan_create/bind/execute/destroy through the C ABI gives
+    the same sigma as the stateless csffci_sigma (general, spin-symmetric
+    and accumulating modes; 1e-12, the scatters' atomic additions may land
+    in another order), and refuses the spin-symmetric mode when created
+    without it."""
+    import ctypes
+    _, D, C = _mods()
+    from pyscf_forge_b200 import _capi
+    from pyscf_forge_b200._runtime import ptr, stream
+    h1, eri = seeded_integrals(norb, 10, seed=21)
+    h2e = D.dev_absorb_h1e(h1, R.restore4(eri, norb), norb, nelec, 0.5)
+    t = C.CSFTransformer(norb, nelec[0], nelec[1], smult)
+    g = torch.Generator(device="cpu").manual_seed(22)
+    c = t.dev_csf2det(torch.randn(t.ncsf, generator=g, dtype=torch.float64).cuda())[0]
+    la, lb = D.dev_link_table(norb, nelec[0]), D.dev_link_table(norb, nelec[1])
+    lib = _capi.load()
+    modes = [(0, 1)]
+    if t.spin_parity is not None:
+        modes.append((_capi.SIGMA_SPIN_SYMMETRIC, t.spin_parity))
+    for flags, eta in modes:
+        nbytes = _capi.query("csffci_sigma_workspace", norb, nelec[0], nelec[1], flags)
+        ws = torch.empty(max(nbytes, 8), dtype=torch.uint8, device="cuda")
+        ref = torch.empty_like(c)
+        _capi.call("csffci_sigma", norb, nelec[0], nelec[1], ptr(h2e), ptr(la), ptr(lb), ptr(c), ptr(ref),
+                   flags, eta, ptr(ws), nbytes, stream())
+        plan = ctypes.c_void_p()
+        need = ctypes.c_size_t()
+        _capi.call("csffci_sigma_plan_create", norb, nelec[0], nelec[1], ptr(h2e), ptr(la), ptr(lb), flags,
+                   ctypes.byref(plan), ctypes.byref(need))
+        try:
+            assert need.value == nbytes
+            pws = torch.empty(max(need.value, 8), dtype=torch.uint8, device="cuda")
+            _capi.call("csffci_sigma_plan_bind", plan, ptr(pws), need.value)
+            got = torch.full_like(c, float("nan"))
+            _capi.call("csffci_sigma_plan_execute", plan, ptr(c), ptr(got), eta, flags, stream())
+            torch.cuda.synchronize()
+            torch.testing.assert_close(got, ref, atol=1e-12, rtol=0)
+            _capi.call("csffci_sigma_plan_execute", plan, ptr(c), ptr(got), eta,
+                       flags | _capi.SIGMA_ACCUMULATE, stream())
+            torch.cuda.synchronize()
+            torch.testing.assert_close(got, 2 * ref, atol=1e-12, rtol=0)
+            if flags == 0 and t.spin_parity is not None:
+                st = lib.csffci_sigma_plan_execute(plan, ptr(c), ptr(got), 1, _capi.SIGMA_SPIN_SYMMETRIC,
+                                                   stream())
+                assert st == _capi.CSFFCI_ERR_INVALID
+        finally:
+            lib.csffci_sigma_plan_destroy(plan)

@@ -5,21 +5,36 @@ deadlocks, no barrier generation mixes two tiles, and no arrival is left
 over at the end.  Barrier ids and counts are those of the kernel: 9 = row
 setup (all warps), 1+s / 4+s = "D of stage s gathered" / "V of stage s
 written" (all warps; one role arrives, the other waits), 7 = movers, 8 = MMA
-warps."""
+warps.
+
+The register-split kernel (pyscf-forge_b200/csrc/sigma_wsr.cu) runs the same
+sequence on 12 MMA warps and 4 movers; four of its MMA warps (the "tail")
+also pass partial sums of the two K halves through a shared buffer indexed
+by the parity of the tile count: the second half writes before barrier 8 of
+the tile, the first half reads after it.  Its model checks that every read
+sees the partial of its own tile."""
 import random
 
 import pytest
 
 
-def _mma_warp(rows):
-    for nch in rows:
+def _mma_warp(rows, tail=None):
+    """tail: None for an MMA warp without partial sums, else (n-tile, K
+    half) of a tail warp of the register-split kernel."""
+    t = 0  # tiles so far (its parity indexes the partial-sum buffer)
+    for r, nch in enumerate(rows):
         for _ in range(4):  # ws_row_setup (3) + after the fold (1)
             yield ("sync", 9, None)
         for c in range(nch):
             s = c % 3
             yield ("sync", 1 + s, ("D", c))
+            if tail is not None and tail[1] == 1:
+                yield ("write", (t & 1, tail[0]), (r, c))
             yield ("sync", 8, None)
+            if tail is not None and tail[1] == 0:
+                yield ("read", (t & 1, tail[0]), (r, c))
             yield ("arrive", 4 + s, ("V", c))
+            t += 1
 
 
 def _mover_warp(rows):
@@ -35,12 +50,14 @@ def _mover_warp(rows):
                 yield ("sync", 4 + (c - 2) % 3, ("V", c - 2))
 
 
-def _run(rows, nwm, nmov, seed):
+def _run(rows, nwm, nmov, seed, tails=()):
     rng = random.Random(seed)
     counts = {9: nwm + nmov, 7: nmov, 8: nwm}
     for s in range(3):
         counts[1 + s] = counts[4 + s] = nwm + nmov
-    warps = [_mma_warp(rows) for _ in range(nwm)] + [_mover_warp(rows) for _ in range(nmov)]
+    warps = ([_mma_warp(rows) for _ in range(nwm - len(tails))] + [_mma_warp(rows, t) for t in tails]
+             + [_mover_warp(rows) for _ in range(nmov)])
+    slots = {}
     cur = [next(w) for w in warps]
     blocked, gen = {}, {b: 0 for b in counts}
     arrived = {b: [] for b in counts}
@@ -57,6 +74,14 @@ def _run(rows, nwm, nmov, seed):
         assert ready, "deadlock"
         i = rng.choice(ready)
         op, bid, tag = cur[i]
+        if op == "write":
+            slots[bid] = tag
+            advance(i)
+            continue
+        if op == "read":
+            assert slots.get(bid) == tag, ("partial sum of another tile", bid, slots.get(bid), tag)
+            advance(i)
+            continue
         arrived[bid].append(tag)
         if op == "sync":
             blocked[i] = (bid, gen[bid])
@@ -79,3 +104,13 @@ def test_ws_barrier_protocol(nwm, nmov):
     for rows in ([1], [2], [3], [1, 4, 2, 7, 3], [5, 1, 1, 6], [10, 9, 8]):
         for seed in range(25):
             _run(rows, nwm, nmov, seed)
+
+
+def test_wsr_tail_partial_sums():
+    """12 MMA warps of which 4 are tail warps ((n-tile, K half) = (0,0),
+    (1,0), (0,1), (1,1)) and 4 movers: the shapes of the register-split
+    kernel at 16 orbitals."""
+    tails = [(0, 0), (1, 0), (0, 1), (1, 1)]
+    for rows in ([1], [2], [3], [1, 4, 2, 7, 3], [5, 1, 1, 6], [10, 9, 8]):
+        for seed in range(40):
+            _run(rows, 12, 4, seed, tails)
