@@ -204,3 +204,24 @@ def test_gas_energies_against_dense_csf_hamiltonian(tag):
         w = np.linalg.eigvalsh(Us @ H @ Us.T)
         e = g["energies_s%d" % sm]
         np.testing.assert_allclose(w[:e.size], e, atol=1e-9)
+
+
+def test_davidson1_restatement_matches_eigh():
+    """The restatement of lib.davidson1 (oracle/davidson_np.py) finds the
+    lowest roots of a symmetric matrix, with the diagonal and the p-space
+    Olsen preconditioners, to 1e-10."""
+    import davidson_np as Dv
+    rng = np.random.default_rng(3)
+    n = 400
+    A = rng.normal(size=(n, n)) * 0.3
+    A = A + A.T + np.diag(np.linspace(0.0, 40.0, n))
+    w = np.linalg.eigvalsh(A)
+    hd = np.diag(A).copy()
+    addr = np.argsort(hd)[:30]
+    pw, pv = np.linalg.eigh(A[np.ix_(addr, addr)])
+    for pre in (Dv.make_diag_precond(hd, 1e-3), Dv.make_pspace_precond(hd, pw, pv, addr, 1e-3)):
+        for nroots in (1, 3):
+            x0 = [np.eye(n)[i] for i in np.argsort(hd)[:nroots]]
+            conv, e, x = Dv.davidson1(lambda v: A @ v, x0, pre, tol=1e-12, nroots=nroots, max_cycle=300)
+            assert all(conv)
+            np.testing.assert_allclose(e, w[:nroots], atol=1e-10)
