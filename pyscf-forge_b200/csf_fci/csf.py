@@ -502,6 +502,46 @@ class FCISolver(CSFFCISolver, FCIBase):
         x = get_init_guess(norb, nelec, nroots, hdiag_csf, self.transformer)
         return self.transformer.dev_csf2det(x)
 
+    # One problem small enough that host round trips would dominate its
+    # Davidson iterations runs them device-resident instead (the batched
+    # solver's plan with one problem: every step on the device, one captured
+    # iteration replayed as a CUDA graph).  Larger problems keep the
+    # host-driven loop, whose sigma is the single-problem warp-specialised
+    # kernel.  Set device_resident = False to always take the host loop.
+    device_resident = True
+    device_resident_max_ncsf = 2000000
+    _DEVICE_KW = {'nroots', 'tol', 'lindep', 'max_cycle', 'max_space', 'pspace_size', 'davidson_only'}
+
+    def _device_resident_ok(self, h1e, eri, norb, nelec, ci0, kwargs):
+        if not self.device_resident or ci0 is not None or not set(kwargs) <= self._DEVICE_KW:
+            return False
+        if not isinstance(h1e, np.ndarray) or h1e.ndim != 2 or isinstance(eri, torch.Tensor):
+            return False
+        if kwargs.get('davidson_only', self.davidson_only):
+            return False
+        nroots = kwargs.get('nroots', self.nroots)
+        t = self.transformer
+        if t is None or t.gas is not None or t.idx_sym is not None or self.gas_orbs is not None:
+            return False
+        return 4 <= norb <= 16 and 1 <= nroots <= 8 and t.ncsf <= self.device_resident_max_ncsf
+
+    def _kernel_device_resident(self, h1e, eri, norb, nelec, kwargs):
+        from ..batched import BatchedCSFSolver, Problem
+        nroots = min(int(kwargs.get('nroots', self.nroots)), self.transformer.ncsf)
+        tol = kwargs.get('tol', self.conv_tol)
+        sol = BatchedCSFSolver(conv_tol=tol, lindep=kwargs.get('lindep', self.lindep),
+                               max_cycle=kwargs.get('max_cycle', self.max_cycle),
+                               max_space=kwargs.get('max_space', self.max_space), level_shift=self.level_shift,
+                               pspace_size=kwargs.get('pspace_size', self.pspace_size),
+                               conv_tol_residual=getattr(self, 'conv_tol_residual', None))
+        p = Problem(norb, _unpack_nelec(nelec, self.spin), self.smult, nroots, h1e, eri)
+        e, cis, _, conv = sol.kernel([p], with_rdm=False)[0]
+        self.converged = conv if nroots == 1 else [conv] * nroots
+        self.niter = int(sol.niter[0]) if sol.niter is not None else 0
+        if nroots > 1:
+            return np.asarray(e), cis
+        return float(e[0]), cis[0]
+
     def kernel(self, h1e, eri, norb, nelec, ci0=None, **kwargs):
         kwargs.pop('max_memory', None)
         self.norb = norb
@@ -509,6 +549,10 @@ class FCISolver(CSFFCISolver, FCIBase):
         if 'smult' in kwargs:
             self.smult = kwargs.pop('smult')
         self.check_transformer_cache()
+        if self._device_resident_ok(h1e, eri, norb, nelec, ci0, kwargs):
+            e, c = self._kernel_device_resident(h1e, eri, norb, nelec, kwargs)
+            self.eci, self.ci = e, c
+            return e, c
         e, c = kernel(self, h1e, eri, norb, nelec, smult=self.smult, idx_sym=None, ci0=ci0,
                       transformer=self.transformer, **kwargs)
         as_torch = isinstance(h1e, torch.Tensor)

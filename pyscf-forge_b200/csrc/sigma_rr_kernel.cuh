@@ -31,6 +31,8 @@ struct RRArgs {
   unsigned off_d, off_l, off_crow, off_al, off_zl, off_pn, off_zf;
   unsigned off_ap;     // warp-specialised kernels: per-pair alpha offsets
   unsigned off_extra;  // register-split kernel: tail partial sums
+  unsigned off_mbar;   // warp-specialised kernels: one mbarrier per stage
+  int bulk;            // warp-specialised kernels: alpha rows by bulk copy
 };
 
 // Alpha link of the current row Ja as the tile loops use it: the offset
@@ -422,9 +424,11 @@ int sigma_ws_launch(int norb, const csffci_sigma_job_t& job0, long long total_un
 // the warp-specialised kernel with registers re-split between the roles
 // (sigma_wsr.cu), one problem at 16 orbitals
 constexpr int RR_VARIANT_WSR = 5;
+// the same with the alpha rows moved by the bulk-copy engine
+constexpr int RR_VARIANT_WSR_BULK = 6;
 bool sigma_wsr_supported(int norb);
 int sigma_wsr_launch(int norb, const csffci_sigma_job_t& job0, long long total_units, long long max_nb,
-                     int max_nla, int max_nlb, cudaStream_t stream);
+                     int max_nla, int max_nlb, cudaStream_t stream, bool bulk);
 bool rr_variant_valid(int norb, int v);
 int rr_default_variant(int norb);
 int sigma_rr_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev, const csffci_sigma_job_t& job0,

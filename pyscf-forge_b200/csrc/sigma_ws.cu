@@ -72,9 +72,14 @@ __global__ void __launch_bounds__(WSLayout<MT>::NTOT * 32, 1) k_sigma_ws(RRArgs 
   S.zf = (int*)(smraw + g.off_zf);
   S.srow = &srow;
   S.apoff = (long long*)(smraw + g.off_ap);
+  S.mbar = (unsigned long long*)(smraw + g.off_mbar);
   const csffci_sigma_job_t& sjob = g.job0;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (g.bulk && tid == 0) {
+    for (int s = 0; s < WS_STAGES; ++s) ws_mbar_init(&S.mbar[s], 1);
+    ws_mbar_init_fence();  // the row setup's barriers order it before every use
+  }
   const int ds = g.ds, npair = g.npair;
   const int ndr = g.nd_rows;
   const size_t dsz = (size_t)ndr * ds;
@@ -217,6 +222,7 @@ size_t ws_layout(RRArgs& g, int npair, int rows_multiple, long long max_nb, int 
   g.off_pn = take((size_t)2 * npair * sizeof(unsigned));
   g.off_zf = take((size_t)npair * sizeof(int));
   g.off_ap = take((size_t)npair * sizeof(long long));  // per-pair alpha offsets
+  g.off_mbar = take((size_t)WS_STAGES * sizeof(unsigned long long));
   if (extra_bytes) {
     const unsigned o = take(extra_bytes);
     if (extra_off) *extra_off = o;

@@ -37,6 +37,49 @@ __device__ __forceinline__ void ws_dmma(double& c0, double& c1, double a, double
 constexpr int WS_NB = 16;     // columns per tile
 constexpr int WS_STAGES = 3;  // ring of D/V and link buffers
 
+// ---- bulk copies of the alpha rows (global -> shared on this GPU, no
+//      multicast), completed on one mbarrier per stage ----------------------
+__device__ __forceinline__ unsigned ws_smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void ws_mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(ws_smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void ws_mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+
+// one arrival that also announces the bytes the stage's copies will deliver
+__device__ __forceinline__ void ws_mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(ws_smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool ws_mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(ws_smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// src and dst 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void ws_bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   ws_smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(ws_smem_addr(bar))
+               : "memory");
+}
+
+// generic-proxy accesses of shared memory before this point are ordered
+// before later async-proxy (bulk copy) accesses
+__device__ __forceinline__ void ws_fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+// try_wait polls allowed before a stage's copies count as lost
+constexpr long long WS_MBAR_POLLS = 1ll << 22;
+
 // The shared state of the row Ja a CTA works on.
 struct WSShared {
   double* Dbuf;
@@ -48,6 +91,7 @@ struct WSShared {
   int* zf;
   RRRow* srow;
   long long* apoff;  // per pair row: Ka*Nb of its alpha link in row Ja, -1 without one
+  unsigned long long* mbar;  // one mbarrier per stage (bulk alpha-row copies)
 };
 
 // Row setup shared by both roles (every thread of the CTA calls it with the
@@ -128,6 +172,7 @@ __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S
   const size_t dsz = (size_t)g.nd_rows * ds, lsz = (size_t)NB * LS;
   const int jl = mtid % NB, ml = mtid / NB;
   int par = 0;
+  unsigned mphase = 0;  // parity to wait for next, per stage (bulk copies)
   for (long long u = blockIdx.x; u < g.total_units; u += gridDim.x) {
     const long long lu = u - sjob.unit_begin;
     for (int w = 0; w < (sjob.sym ? 2 : 1); ++w) {
@@ -154,7 +199,24 @@ __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S
           csffci_link_t* Ld = S.Lbuf + s * lsz;
           const long long j1 = (long long)c * NB;
           const int nc = (int)min((long long)NB, jend - j1);
-          if (jl < nc) {
+          if (g.bulk) {
+            // one mover warp hands the alpha rows of tile c to the bulk-copy
+            // engine: row l is c[Ka_l][j1 .. j1+nc) rounded up to an even
+            // count (16-byte size; the extra column is in bounds because Nb
+            // is even and only lands in a column the scatters skip)
+            if (mwarp == 0) {
+              const unsigned rowbytes = (unsigned)((nc + 1) & ~1) * 8u;
+              if (lane == 0) {
+                ws_fence_proxy_async();
+                ws_mbar_expect_tx(&S.mbar[s], rowbytes * (unsigned)nla);
+              }
+              __syncwarp();
+              for (int l = lane; l < nla; l += 32) {
+                const RRAlpha a = S.al[l];
+                ws_bulk_g2s(&Dd[a.drow], sjob.ci + a.off + j1, rowbytes, &S.mbar[s]);
+              }
+            }
+          } else if (jl < nc) {
             const double* src = sjob.ci + j1 + jl;
             for (int l0 = ml; l0 < nla; l0 += RU * MPASS) {
               RRAlpha a[RU];
@@ -178,8 +240,21 @@ __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S
           // tile c, may still be in flight)
           if (c < nch) cp_async_wait_one();
           else cp_async_wait_all();
-          ws_bar_sync(7, MTH);
           const int s = (c - 1) % WS_STAGES;
+          if (g.bulk) {
+            // the alpha rows of tile c-1 have landed (bounded wait: a stage
+            // whose copies never complete poisons this row's sigma with NaN
+            // and the kernel goes on, so that no barrier is left waiting)
+            const unsigned parity = (mphase >> s) & 1u;
+            long long polls = 0;
+            while (!ws_mbar_try_wait(&S.mbar[s], parity))
+              if (++polls > WS_MBAR_POLLS) {
+                if (mtid == 0) atomicAdd(&(SYM ? sjob.scratch : sjob.sigma)[ja * Nb], __longlong_as_double(0x7ff8000000000000ll));
+                break;
+              }
+            mphase ^= 1u << s;
+          }
+          ws_bar_sync(7, MTH);
           double* D = S.Dbuf + s * dsz;
           const csffci_link_t* Lt = S.Lbuf + s * lsz;
           const int ncol = (int)min((long long)NB, jend - (long long)(c - 1) * NB);
@@ -205,6 +280,7 @@ __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S
               for (int k = 0; k < RU; ++k)
                 if (m0 + k * MPASS < nlb) D[rr_lpair(e[k]) * ds + jl] = d[k] + rr_flip(v[k], f[k]);
             }
+          if (g.bulk) ws_fence_proxy_async();
           ws_bar_arrive(1 + s, NTH);  // D of tile c-1 is gathered
         }
         if (c >= 2) {
@@ -243,5 +319,11 @@ __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S
 // offset returned in *extra_off).  Returns 0 when it does not fit.
 size_t ws_layout(RRArgs& g, int npair, int rows_multiple, long long max_nb, int max_nla, int max_nlb,
                  size_t extra_bytes, unsigned* extra_off);
+
+// whether the alpha rows of one problem can go through the bulk-copy
+// engine: 16-byte aligned rows of c (ci 16-byte aligned, Nb even)
+inline bool ws_bulk_ok(const csffci_sigma_job_t& J) {
+  return ((uintptr_t)J.ci & 15u) == 0 && (J.Nb & 1) == 0;
+}
 
 }  // namespace csffci

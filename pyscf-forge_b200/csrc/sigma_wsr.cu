@@ -49,8 +49,8 @@ constexpr int WSR_NTH = WSR_NW * 32;
 constexpr int WSR_NMMA = (WSR_NBIG + WSR_NTAIL) * 32;
 constexpr int WSR_REG_LAUNCH = 128;
 constexpr int WSR_REG_BIG = 176;
-constexpr int WSR_REG_TAIL = 112;
-constexpr int WSR_REG_MOV = 48;
+constexpr int WSR_REG_TAIL = 104;
+constexpr int WSR_REG_MOV = 56;
 constexpr int WSR_RU = 3;  // mover links per pass: 8 link rows per pass x 3 = 24 divides 72
 static_assert(WSR_NTH * WSR_REG_LAUNCH == 65536, "the launch takes the whole register file");
 static_assert(2 * 128 * WSR_REG_BIG + 128 * WSR_REG_TAIL + 128 * WSR_REG_MOV <= WSR_NTH * WSR_REG_LAUNCH,
@@ -85,11 +85,16 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
   S.zf = (int*)(smraw + g.off_zf);
   S.srow = &srow;
   S.apoff = (long long*)(smraw + g.off_ap);
+  S.mbar = (unsigned long long*)(smraw + g.off_mbar);
   // tail partial sums: [tile parity][n-tile][64 doubles]
   double* const Pbuf = (double*)(smraw + g.off_extra);
   const csffci_sigma_job_t& sjob = g.job0;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (g.bulk && tid == 0) {
+    for (int s = 0; s < WS_STAGES; ++s) ws_mbar_init(&S.mbar[s], 1);
+    ws_mbar_init_fence();  // the row setup's barriers order it before every use
+  }
   const int ds = g.ds, npair = g.npair;
   const int ndr = g.nd_rows;
   const size_t dsz = (size_t)ndr * ds;
@@ -160,6 +165,7 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
             V[r1 * ds + 8] = acc[1][2];
             V[r1 * ds + 9] = acc[1][3];
           }
+          if (g.bulk) ws_fence_proxy_async();  // V before the stage's next bulk copy
           ws_bar_arrive(4 + s, WSR_NTH);  // V of tile c is written
           // alpha scatter of this lane's two pair rows from the accumulators
           // (J < Ja in the spin-symmetric mode, whose column Ja is left to
@@ -240,6 +246,7 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
               V[1] = acc1;
             }
           }
+          if (g.bulk) ws_fence_proxy_async();
           ws_bar_arrive(4 + s, WSR_NTH);  // V of tile c is written
           if (!kh) {
             const long long aoff = rt < npair ? S.apoff[rt] : -1;
@@ -266,7 +273,7 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
 bool sigma_wsr_supported(int norb) { return norb == 16; }
 
 int sigma_wsr_launch(int norb, const csffci_sigma_job_t& job0, long long total_units, long long max_nb,
-                     int max_nla, int max_nlb, cudaStream_t stream) {
+                     int max_nla, int max_nlb, cudaStream_t stream, bool bulk) {
   if (!sigma_wsr_supported(norb)) {
     set_error("sigma: the register-split warp-specialised variant covers norb 16, not %d", norb);
     return CSFFCI_ERR_INVALID;
@@ -290,6 +297,7 @@ int sigma_wsr_launch(int norb, const csffci_sigma_job_t& job0, long long total_u
     return CSFFCI_ERR_INVALID;
   }
   g.off_extra = extra;
+  g.bulk = bulk && ws_bulk_ok(job0) ? 1 : 0;
   auto kern = k_sigma_wsr<KS>;
   // setmaxnreg re-splits the registers the launch allocated (128 per
   // thread); with any other count the raise of warpgroups 0-1 could not be
@@ -313,7 +321,7 @@ int sigma_wsr_launch(int norb, const csffci_sigma_job_t& job0, long long total_u
   long long grid = nsm;
   if (grid > g.total_units) grid = g.total_units;
   if (grid < 1) return CSFFCI_OK;
-  ProfScope ps("k_sigma_wsr", stream);
+  ProfScope ps(g.bulk ? "k_sigma_wsr_bulk" : "k_sigma_wsr", stream);
   kern<<<(int)grid, WSR_NTH, smem, stream>>>(g);
   return check_launch("sigma (register-split warp-specialised)");
 }

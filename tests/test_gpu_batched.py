@@ -115,3 +115,30 @@ def test_device_engine_matches_host_engine_and_graph_replay():
         np.testing.assert_allclose(a[0], c[0], atol=1e-10)
     assert sg.tile_variants and all(0 <= v < 4 for v in sg.tile_variants.values())
     assert set(sg.tile_variants) <= {p.norb for p in probs}
+
+
+def test_c3_batch_energies_vs_reference():
+    """The benchmark's 128-problem uneven batch (C3) through the device
+    batched solver, against the energies of the reference's own csf.py
+    kernel on the stand-in (tests/golden/c3_batch128.npz, made by
+    tests/golden/make_c3_golden.py with the same solver settings): the
+    batch generator makes the fixture's problems, every problem converges,
+    and every root is within 1e-9 Eh of the reference."""
+    import os
+    from conftest import GOLDEN
+    path = os.path.join(GOLDEN, "c3_batch128.npz")
+    if not os.path.exists(path):
+        pytest.skip("C3 fixture not generated")
+    from pyscf_forge_b200 import batched as B
+    g = np.load(path)
+    conv_tol, max_cycle, max_space = g["settings"]
+    probs = B.make_uneven_batch(128)
+    got = np.array([(i, p.norb, p.nelec[0], p.nelec[1], p.smult, p.nroots) for i, p in enumerate(probs)])
+    assert np.array_equal(got, g["problems"])
+    assert g["converged"].all()
+    sol = B.BatchedCSFSolver(conv_tol=float(conv_tol), max_cycle=int(max_cycle), max_space=int(max_space))
+    res = sol.kernel(probs, with_rdm=False)
+    for i, r in enumerate(res):
+        e = np.asarray(r[0])
+        assert bool(np.all(r[3])), ("problem %d not converged" % i)
+        np.testing.assert_allclose(e, g["energies"][i, :len(e)], atol=1e-9, err_msg="problem %d" % i)

@@ -430,7 +430,10 @@ def test_solver_contract_2e_out_buffers():
                                              (16, (3, 2), 8)])
 def test_warp_specialised_sigma(norb, nelec, rank, monkeypatch):
     """The warp-specialised sigma kernels (tile variant 4 from 13 orbitals,
-    variant 5 -- registers re-split between the roles -- at 16): against the
+    variant 5 -- registers re-split between the roles -- and variant 6 --
+    the same with the alpha rows moved by the bulk-copy engine -- at 16;
+    variant 6 also from a vector 8 bytes off 16-byte alignment, which it
+    copies element by element instead): against the
     reference C (1e-10) and against the phase-serial kernel (1e-12), in the
     general mode and, for na == nb, the spin-symmetric mode with a symmetric
     (eta = +1) and an antisymmetric (eta = -1) vector."""
@@ -446,7 +449,7 @@ def test_warp_specialised_sigma(norb, nelec, rank, monkeypatch):
     cases = [(c0, (None,))]
     if na == nb:
         cases = [(c0 + c0.T, (None, 1)), (c0 - c0.T, (-1,))]
-    variants = (4, 5) if norb == 16 else (4,)
+    variants = (4, 5, 6) if norb == 16 else (4,)
     for c, etas in cases:
         c = c / np.linalg.norm(c)
         ref = gasref.contract_2e(h2e_np, c, norb, nelec).ravel()
@@ -459,6 +462,11 @@ def test_warp_specialised_sigma(norb, nelec, rank, monkeypatch):
                 ws = D.dev_contract_2e(h2e, cd, norb, nelec, eta=eta).cpu().numpy()
                 np.testing.assert_allclose(ws, ref, atol=1e-10)
                 np.testing.assert_allclose(ws, rr, atol=1e-12)
+                if v == 6:
+                    buf = torch.empty(cd.numel() + 1, dtype=torch.float64, device="cuda")
+                    buf[1:] = cd
+                    ws = D.dev_contract_2e(h2e, buf[1:], norb, nelec, eta=eta).cpu().numpy()
+                    np.testing.assert_allclose(ws, rr, atol=1e-12)
     monkeypatch.delenv("CSFFCI_SIGMA_VARIANT")
 
 
