@@ -3,6 +3,7 @@
 // (rdm.cu).  All reductions are done in a fixed order (per-block partials,
 // then one ordered pass) so results are bit-reproducible run to run.
 #include "common.cuh"
+#include "profile.cuh"
 
 namespace csffci {
 
@@ -108,7 +109,10 @@ int csffci_combine(int ny, double* y, int64_t ldy, double beta, int nx, const do
   CSF_REQUIRE(ny >= 0 && nx >= 0 && n >= 0 && nx * ny <= 4096, "combine: bad sizes");
   if (ny == 0 || n == 0) return CSFFCI_OK;
   size_t sm = (size_t)nx * ny * sizeof(double);
-  k_combine<<<grid_for(n, 256, 148 * 8), 256, sm, stream>>>(ny, y, ldy, beta, nx, x, ldx, coef, n);
+  {
+    ProfScope ps_("k_combine", stream);
+    k_combine<<<grid_for(n, 256, 148 * 8), 256, sm, stream>>>(ny, y, ldy, beta, nx, x, ldx, coef, n);
+  }
   return check_launch("combine");
 }
 
@@ -118,7 +122,10 @@ int csffci_precond_dots(int64_t n, const double* r, const double* x, const doubl
                         double shift, double* out2, double* work, cudaStream_t stream) {
   CSF_REQUIRE(n >= 0 && work != nullptr && out2 != nullptr, "precond_dots: bad arguments");
   int nblk = grid_for(n > 0 ? n : 1, 256, 148 * 4);
-  k_precond_dots<<<nblk, 256, 0, stream>>>(n, r, x, hdiag, e, shift, work);
+  {
+    ProfScope ps_("k_precond_dots", stream);
+    k_precond_dots<<<nblk, 256, 0, stream>>>(n, r, x, hdiag, e, shift, work);
+  }
   int st = check_launch("precond dots");
   if (st) return st;
   k_precond_sum<<<1, 32, 0, stream>>>(work, nblk, out2);
@@ -132,12 +139,18 @@ int csffci_precond(int64_t n, const double* r, const double* x, const double* hd
   if (n == 0) return CSFFCI_OK;
   int nblk = grid_for(n, 256, 148 * 4);
   if (mode == 1) {
-    k_precond_dots<<<nblk, 256, 0, stream>>>(n, r, x, hdiag, e, shift, work);
+    {
+      ProfScope ps_("k_precond_dots", stream);
+      k_precond_dots<<<nblk, 256, 0, stream>>>(n, r, x, hdiag, e, shift, work);
+    }
     int st = check_launch("precond dots");
     if (st) return st;
   }
-  k_precond_apply<<<grid_for(n, 256, 148 * 8), 256, 0, stream>>>(n, r, x, hdiag, e, shift, mode, e1,
-                                                                work, nblk, t);
+  {
+    ProfScope ps_("k_precond_apply", stream);
+    k_precond_apply<<<grid_for(n, 256, 148 * 8), 256, 0, stream>>>(n, r, x, hdiag, e, shift, mode, e1,
+                                                                  work, nblk, t);
+  }
   return check_launch("precond");
 }
 

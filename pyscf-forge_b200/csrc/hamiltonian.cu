@@ -3,6 +3,7 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "profile.cuh"
 
 namespace csffci {
 
@@ -248,8 +249,11 @@ int csffci_hdiag_det(int norb, int neleca, int nelecb, const double* h1a, const 
                                                                     eri, eb, nullptr, sb);
   st = check_launch("hdiag_det beta strings");
   if (st) return st;
-  k_hdiag_det<<<grid_for((long long)(Na * Nb), 256, 148 * 32), 256, 0, stream>>>(norb, Na, Nb, ea,
-                                                                                  eb, ja, sb, hdiag);
+  {
+    ProfScope ps_("k_hdiag_det", stream);
+    k_hdiag_det<<<grid_for((long long)(Na * Nb), 256, 148 * 32), 256, 0, stream>>>(norb, Na, Nb, ea,
+                                                                                    eb, ja, sb, hdiag);
+  }
   return check_launch("hdiag_det");
 }
 
@@ -260,8 +264,11 @@ int csffci_pspace_h0(int norb, int neleca, int nelecb, const double* h1a, const 
   if (n == 0) return CSFFCI_OK;
   int npair = norb * (norb + 1) / 2;
   unsigned long long Nb = host_binom(norb, nelecb);
-  k_pspace_h0<<<grid_for((long long)n * n, 128, 148 * 32), 128, 0, stream>>>(
-      norb, npair, Nb, h1a, h1b, eri, hdiag_det, det_addr, neleca, nelecb, n, h0);
+  {
+    ProfScope ps_("k_pspace_h0", stream);
+    k_pspace_h0<<<grid_for((long long)n * n, 128, 148 * 32), 128, 0, stream>>>(
+        norb, npair, Nb, h1a, h1b, eri, hdiag_det, det_addr, neleca, nelecb, n, h0);
+  }
   return check_launch("pspace_h0");
 }
 

@@ -96,8 +96,11 @@ int gram_run(int nx, const double* x, int64_t ldx, int ny, const double* y, int6
   nsplit = (int)((n + kchunk - 1) / kchunk);
   if (nsplit < 1) nsplit = 1;
   int tiles = ((nx + GT - 1) / GT) * ((ny + GT - 1) / GT);
-  k_gram_part<<<grid_for((int64_t)tiles * nsplit, 1, 148 * 8), 256, 0, stream>>>(
-      nx, x, ldx, ny, y, ldy, n, kchunk, nsplit, part);
+  {
+    ProfScope ps_("k_gram_part", stream);
+    k_gram_part<<<grid_for((int64_t)tiles * nsplit, 1, 148 * 8), 256, 0, stream>>>(
+        nx, x, ldx, ny, y, ldy, n, kchunk, nsplit, part);
+  }
   int st = check_launch("gram");
   if (st) return st;
   k_gram_reduce<<<grid_for(nx * ny, 256), 256, 0, stream>>>(nx * ny, nsplit, part, out, accumulate);

@@ -62,7 +62,10 @@ int sigma_rr_single_variant(int norb) {
     if (rr_variant_valid(norb, v)) return v;
   }
   // measured on B200 (singlet, one problem): 14 orbitals 7.61 -> 6.31 ms,
-  // 15: 31.1 -> 25.8 ms, 16: 148.8 -> 129.5 ms; at 13 it is no faster
+  // 15: 31.1 -> 25.8 ms, 16: 148.8 -> 129.5 ms (k_sigma_ws) and 119 ms
+  // (k_sigma_wsr, registers re-split between the roles); at 13 the
+  // warp-specialised kernel is no faster
+  if (sigma_wsr_supported(norb)) return RR_VARIANT_WSR;
   return norb >= 14 && sigma_ws_supported(norb) ? RR_VARIANT_WS : -1;
 }
 

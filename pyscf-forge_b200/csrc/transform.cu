@@ -8,6 +8,7 @@
 // permutation, so the scatter has no conflicts.  HBM-bound: every CI element
 // is read once and written once per call.
 #include "common.cuh"
+#include "profile.cuh"
 
 namespace csffci {
 
@@ -152,7 +153,10 @@ static int run_blocks(int nvec, const double* x, int64_t ldx, double* y, int64_t
     int64_t M = (int64_t)nvec * B.nconf;
     int N = (MODE == MODE_DET2CSF) ? B.ncsf : B.ndet;
     int64_t tiles = ((M + TBM - 1) / TBM) * ((N + TBN - 1) / TBN);
-    k_block_gemm<MODE><<<grid_for(tiles, 1, 148 * 8), 256, 0, stream>>>(g);
+    {
+      ProfScope ps_("k_block_gemm", stream);
+      k_block_gemm<MODE><<<grid_for(tiles, 1, 148 * 8), 256, 0, stream>>>(g);
+    }
     int st = check_launch("det/csf transform");
     if (st) return st;
   }
@@ -241,8 +245,11 @@ int csffci_csf2det(int nvec, const double* x_csf, int64_t ld_csf, double* x_det,
   for (int b = 0; b < nblock; ++b)
     if ((blocks[b].ncsf == 0 && blocks[b].nconf > 0) || blocks[b].conf_sel != nullptr) full = false;
   if (!full) {
-    k_zero_rows<<<grid_for((int64_t)nvec * ndet, 256, 148 * 16), 256, 0, stream>>>(x_det, ld_det,
-                                                                                     nvec, ndet);
+    {
+      ProfScope ps_("k_zero_rows", stream);
+      k_zero_rows<<<grid_for((int64_t)nvec * ndet, 256, 148 * 16), 256, 0, stream>>>(x_det, ld_det,
+                                                                                       nvec, ndet);
+    }
     int st = check_launch("csf2det zero");
     if (st) return st;
   }
@@ -278,7 +285,10 @@ int csffci_hdiag_csf(int norb, int neleca, int nelecb, const double* hdiag_det, 
     g.npair = B.npair;
     g.norb = norb;
     g.npair_orb = npair_orb;
-    k_hdiag_csf<<<grid_for(B.nconf * B.ncsf, 128, 148 * 32), 128, 0, stream>>>(g);
+    {
+      ProfScope ps_("k_hdiag_csf", stream);
+      k_hdiag_csf<<<grid_for(B.nconf * B.ncsf, 128, 148 * 32), 128, 0, stream>>>(g);
+    }
     int st = check_launch("hdiag_csf");
     if (st) return st;
   }
