@@ -407,7 +407,7 @@ def run_rdm(dmma_peak, cases=None):
 
 
 C4_MAX_SPACE = 40
-C4_MAX_CYCLE = 200
+C4_MAX_CYCLE = 100
 
 
 def run_c4(ref_check=True):
@@ -477,7 +477,7 @@ def run_c4(ref_check=True):
     for k, c in enumerate(sol.ci):
         c = c.reshape(-1)
         hc = D.dev_contract_2e(h2e, c, norb, nelec)
-        res.append(float(torch.linalg.norm(hc - float(E[k]) * c)))
+        res.append(float(torch.linalg.norm(hc - float(E[k].detach()) * c)))
         del hc
     out["residual_norms"] = res
     if ref_check:
@@ -488,8 +488,8 @@ def run_c4(ref_check=True):
         plan.close()
         e0 = float(np.dot(c0, hc0) / np.dot(c0, c0))
         out["reference_check_root0"] = {
-            "rayleigh_quotient_minus_e0": e0 - float(E[0]),
-            "residual_norm": float(np.linalg.norm(hc0 - float(E[0]) * c0)),
+            "rayleigh_quotient_minus_e0": e0 - float(E[0].detach()),
+            "residual_norm": float(np.linalg.norm(hc0 - float(E[0].detach()) * c0)),
             "note": "the reference's CPU sigma (libfci_gas, one GAS subspace) applied to root 0"}
     return out
 
@@ -572,10 +572,14 @@ def main():
     ap.add_argument("--no-rdm", action="store_true", help="skip the RDM (adjoint) timing")
     ap.add_argument("--no-c4", action="store_true", help="skip the CAS(16,16) 4-root solve + RDM backward")
     ap.add_argument("--c4-only", action="store_true", help="only the CAS(16,16) 4-root solve + RDM backward")
+    ap.add_argument("--c4-max-cycle", type=int, default=None, help="Davidson iterations of the C4 solve")
     ap.add_argument("--rdm-only", default="", help="only the RDM timing of these cases "
                     "(cas16_singlet_1root,cas14_sa2), for profiling captures")
     ap.add_argument("--batch", type=int, default=128, help="problems in the batched-solves measurement")
     args = ap.parse_args()
+    global C4_MAX_CYCLE
+    if args.c4_max_cycle:
+        C4_MAX_CYCLE = args.c4_max_cycle
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":

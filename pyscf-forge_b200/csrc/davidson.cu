@@ -7,25 +7,35 @@
 
 namespace csffci {
 
-// y[r][k] = beta*y[r][k] + sum_i coef[r][i] x[i][k]
+// y[r][k] = beta*y[r][k] + sum_i coef[r][i] x[i][k]: rows of y in groups of
+// CB_RG held in registers, x read once per group (coalesced over k, the
+// loop over i unrolled so that several loads are in flight); each output is
+// beta*y first, then the terms in ascending i (a fixed order)
+constexpr int CB_RG = 4;
 __global__ void k_combine(int ny, double* y, int64_t ldy, double beta, int nx,
                           const double* __restrict__ x, int64_t ldx, const double* __restrict__ coef,
                           int64_t n) {
-  extern __shared__ double cs[];
-  for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) cs[i] = coef[i];
+  extern __shared__ double cs[];  // coef rows padded with zeros to a multiple of CB_RG
+  const int nyp = (ny + CB_RG - 1) / CB_RG * CB_RG;
+  for (int i = threadIdx.x; i < nx * nyp; i += blockDim.x) cs[i] = i < nx * ny ? coef[i] : 0.0;
   __syncthreads();
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
        k += (int64_t)gridDim.x * blockDim.x) {
-    double xv[32];
-    for (int i0 = 0; i0 < nx; i0 += 32) {
-      int m = nx - i0 < 32 ? nx - i0 : 32;
-      for (int i = 0; i < m; ++i) xv[i] = x[(int64_t)(i0 + i) * ldx + k];
-      for (int r = 0; r < ny; ++r) {
-        double acc = (i0 == 0) ? (beta == 0.0 ? 0.0 : beta * y[(int64_t)r * ldy + k])
-                               : y[(int64_t)r * ldy + k];
-        for (int i = 0; i < m; ++i) acc = fma(cs[r * nx + i0 + i], xv[i], acc);
-        y[(int64_t)r * ldy + k] = acc;
+    for (int r0 = 0; r0 < ny; r0 += CB_RG) {
+      double acc[CB_RG];
+#pragma unroll
+      for (int rr = 0; rr < CB_RG; ++rr)
+        acc[rr] = (r0 + rr < ny && beta != 0.0) ? beta * y[(int64_t)(r0 + rr) * ldy + k] : 0.0;
+      const double* c0 = cs + (int64_t)r0 * nx;
+#pragma unroll 8
+      for (int i = 0; i < nx; ++i) {
+        const double xv = x[(int64_t)i * ldx + k];
+#pragma unroll
+        for (int rr = 0; rr < CB_RG; ++rr) acc[rr] = fma(c0[rr * nx + i], xv, acc[rr]);
       }
+#pragma unroll
+      for (int rr = 0; rr < CB_RG; ++rr)
+        if (r0 + rr < ny) y[(int64_t)(r0 + rr) * ldy + k] = acc[rr];
     }
   }
 }
@@ -106,9 +116,10 @@ extern "C" {
 
 int csffci_combine(int ny, double* y, int64_t ldy, double beta, int nx, const double* x,
                    int64_t ldx, const double* coef, int64_t n, cudaStream_t stream) {
-  CSF_REQUIRE(ny >= 0 && nx >= 0 && n >= 0 && nx * ny <= 4096, "combine: bad sizes");
+  CSF_REQUIRE(ny >= 0 && nx >= 0 && n >= 0 && nx * ((ny + CB_RG - 1) / CB_RG * CB_RG) <= 4096,
+              "combine: bad sizes");
   if (ny == 0 || n == 0) return CSFFCI_OK;
-  size_t sm = (size_t)nx * ny * sizeof(double);
+  size_t sm = (size_t)nx * ((ny + CB_RG - 1) / CB_RG * CB_RG) * sizeof(double);
   {
     ProfScope ps_("k_combine", stream);
     k_combine<<<grid_for(n, 256, 148 * 8), 256, sm, stream>>>(ny, y, ldy, beta, nx, x, ldx, coef, n);

@@ -8,10 +8,135 @@
 // (conventions of pyscf/lib/mcscf/fci_gas.h:260-268).  The determinant
 // space is processed in slabs that fit the caller's workspace, so D(pq,J)
 // is never materialised for the whole space.
+#include <utility>
+
 #include "common.cuh"
 #include "profile.cuh"
 
 namespace csffci {
+
+// ---------------------------------------------------------------------------
+// skinny Gram for the Davidson projections: out[i][j] = sum_k X[i][k] Y[j][k]
+// with at most GS_MAXY vectors on one side (the new corrections or the Ritz
+// vectors) and at most GS_MAXX on the other (the subspace).  Each block
+// streams k-chunks of GS_NT*KT elements: the chunk of the narrow side stays
+// in registers while every row of the wide side is read once (coalesced,
+// KT loads per thread), so the kernel moves (nx + ny) * n * 8 bytes and is
+// bound by HBM bandwidth.  Per-warp sums accumulate in shared memory in a
+// fixed order; the block partials are summed over the blocks in a fixed
+// order as well, so results are bit-reproducible.
+// ---------------------------------------------------------------------------
+constexpr int GS_NT = 256, GS_MAXX = 64, GS_MAXY = 4;
+
+template <int NY, int KT>
+__global__ void __launch_bounds__(GS_NT) k_gram_skinny(int nx, const double* __restrict__ x, int64_t ldx, int ny,
+                                                       const double* __restrict__ y, int64_t ldy, int64_t n,
+                                                       double* part) {
+  __shared__ double wsum[GS_NT / 32][GS_MAXX][NY];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int e = lane; e < GS_MAXX * NY; e += 32) (&wsum[warp][0][0])[e] = 0.0;
+  __syncwarp();
+  constexpr int KC = GS_NT * KT;
+  for (int64_t k0 = (int64_t)blockIdx.x * KC; k0 < n; k0 += (int64_t)gridDim.x * KC) {
+    double yv[NY][KT];
+#pragma unroll
+    for (int q = 0; q < KT; ++q) {
+      const int64_t k = k0 + tid + (int64_t)q * GS_NT;
+#pragma unroll
+      for (int j = 0; j < NY; ++j) yv[j][q] = (j < ny && k < n) ? y[(int64_t)j * ldy + k] : 0.0;
+    }
+    for (int i = 0; i < nx; ++i) {
+      const double* xi = x + (int64_t)i * ldx;
+      double sj[NY];
+#pragma unroll
+      for (int j = 0; j < NY; ++j) sj[j] = 0.0;
+#pragma unroll
+      for (int q = 0; q < KT; ++q) {
+        const int64_t k = k0 + tid + (int64_t)q * GS_NT;
+        const double xv = k < n ? xi[k] : 0.0;
+#pragma unroll
+        for (int j = 0; j < NY; ++j) sj[j] = fma(xv, yv[j][q], sj[j]);
+      }
+#pragma unroll
+      for (int j = 0; j < NY; ++j) {
+        double v = sj[j];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        sj[j] = v;
+      }
+      if (lane == 0) {
+#pragma unroll
+        for (int j = 0; j < NY; ++j) wsum[warp][i][j] += sj[j];
+      }
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < nx * NY; e += GS_NT) {
+    const int i = e / NY, j = e - i * NY;
+    double v = 0.0;
+#pragma unroll
+    for (int w = 0; w < GS_NT / 32; ++w) v += wsum[w][i][j];
+    part[(int64_t)blockIdx.x * nx * NY + e] = v;
+  }
+}
+
+// out[i][j] (or out[j][i] when transposed) = sum over the blocks of part
+__global__ void k_gram_skinny_reduce(int nx, int ny, int ystride, int nblk, const double* part, double* out,
+                                     int transposed) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nx * ny; e += gridDim.x * blockDim.x) {
+    const int i = e / ny, j = e - i * ny;
+    double v = 0.0;
+    for (int b = 0; b < nblk; ++b) v += part[((int64_t)b * nx + i) * ystride + j];
+    if (transposed)
+      out[(int64_t)j * nx + i] = v;
+    else
+      out[e] = v;
+  }
+}
+
+static int gram_skinny_ystride(int ny) { return ny <= 1 ? 1 : ny <= 2 ? 2 : 4; }
+
+static int gram_skinny_blocks(int64_t n, int ny) {
+  const int kt = ny <= 2 ? 16 : 8;
+  int64_t nb = (n + GS_NT * kt - 1) / (GS_NT * kt);
+  if (nb > 148 * 4) nb = 148 * 4;
+  return (int)(nb < 1 ? 1 : nb);
+}
+
+static bool gram_skinny_fits(int nx, int ny) {
+  return (ny <= GS_MAXY && nx <= GS_MAXX) || (nx <= GS_MAXY && ny <= GS_MAXX);
+}
+
+static size_t gram_skinny_workspace(int nx, int ny, int64_t n) {
+  if (!(ny <= GS_MAXY && nx <= GS_MAXX)) std::swap(nx, ny);
+  return (size_t)gram_skinny_blocks(n, ny) * nx * gram_skinny_ystride(ny) * sizeof(double);
+}
+
+static int gram_skinny_run(int nx, const double* x, int64_t ldx, int ny, const double* y, int64_t ldy, int64_t n,
+                           double* out, double* part, cudaStream_t stream) {
+  int transposed = 0;
+  if (!(ny <= GS_MAXY && nx <= GS_MAXX)) {
+    std::swap(nx, ny);
+    std::swap(x, y);
+    std::swap(ldx, ldy);
+    transposed = 1;
+  }
+  const int nblk = gram_skinny_blocks(n, ny);
+  const int ys = gram_skinny_ystride(ny);
+  {
+    ProfScope ps_("k_gram_skinny", stream);
+    if (ys == 1)
+      k_gram_skinny<1, 16><<<nblk, GS_NT, 0, stream>>>(nx, x, ldx, ny, y, ldy, n, part);
+    else if (ys == 2)
+      k_gram_skinny<2, 16><<<nblk, GS_NT, 0, stream>>>(nx, x, ldx, ny, y, ldy, n, part);
+    else
+      k_gram_skinny<4, 8><<<nblk, GS_NT, 0, stream>>>(nx, x, ldx, ny, y, ldy, n, part);
+  }
+  int st = check_launch("gram (skinny)");
+  if (st) return st;
+  k_gram_skinny_reduce<<<grid_for(nx * ny, 128), 128, 0, stream>>>(nx, ny, ys, nblk, part, out, transposed);
+  return check_launch("gram (skinny) reduce");
+}
 
 // ---------------------------------------------------------------------------
 // split-K Gram: part[split][i][j] = sum_{k in split} X[i][k] Y[j][k]
@@ -408,15 +533,18 @@ int csffci_gram(int nx, const double* x, int64_t ldx, int ny, const double* y, i
                 int64_t n, double* out, void* work, size_t work_bytes, cudaStream_t stream) {
   CSF_REQUIRE(nx >= 0 && ny >= 0 && n >= 0, "gram: bad sizes");
   if (nx == 0 || ny == 0) return CSFFCI_OK;
-  size_t need = gram_workspace(nx, ny, n);
+  size_t need = csffci_gram_workspace(nx, ny, n);
   if (work == nullptr || work_bytes < need) {
     set_error("gram: workspace of %zu bytes < %zu required", work_bytes, need);
     return CSFFCI_ERR_MEMORY;
   }
+  if (gram_skinny_fits(nx, ny)) return gram_skinny_run(nx, x, ldx, ny, y, ldy, n, out, (double*)work, stream);
   return gram_run(nx, x, ldx, ny, y, ldy, n, out, 0, (double*)work, stream);
 }
 
-size_t csffci_gram_workspace(int nx, int ny, int64_t n) { return gram_workspace(nx, ny, n); }
+size_t csffci_gram_workspace(int nx, int ny, int64_t n) {
+  return gram_skinny_fits(nx, ny) ? gram_skinny_workspace(nx, ny, n) : gram_workspace(nx, ny, n);
+}
 
 size_t csffci_rdm12_workspace(int norb, int neleca, int nelecb) {
   long long ndet = (long long)(host_binom(norb, neleca) * host_binom(norb, nelecb));

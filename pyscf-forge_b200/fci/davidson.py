@@ -86,6 +86,62 @@ class DiagPrecond:
         return t
 
 
+def _orthonormalise_per_vector(V, m, new, lindep):
+    """Append the vectors of new to V[m:] one at a time, each orthogonalised
+    (two passes) against V[:m] and the ones already appended, dropping those
+    whose remaining squared norm is below lindep; returns their rows."""
+    added = []
+    for i in range(new.shape[0]):
+        t = new[i:i + 1].clone()
+        for _ in range(2):
+            if m + len(added):
+                cf = gram(V[:m + len(added)], t).cpu().numpy().T
+                combine(t, V[:m + len(added)], -cf, beta=1.0)
+        nrm2 = float(gram(t, t).cpu().numpy()[0, 0])
+        if nrm2 > lindep:
+            V[m + len(added)].copy_(t[0] / np.sqrt(nrm2))
+            added.append(m + len(added))
+    return added
+
+
+def _orthonormalise_into(V, m, new, lindep):
+    """The same result as _orthonormalise_per_vector for a block of new
+    vectors, with the subspace read once per pass: two passes of block
+    Gram-Schmidt against V[:m] (one Gram block and one combine each), then
+    Gram-Schmidt among the block on its small Gram matrix (host), checked:
+    if the appended block is not orthonormal to 1e-8 the per-vector form
+    runs instead."""
+    k = new.shape[0]
+    if k == 1:
+        return _orthonormalise_per_vector(V, m, new, lindep)
+    T = new.clone()
+    for _ in range(2):
+        if m:
+            cf = gram(V[:m], T).cpu().numpy()          # (m, k)
+            combine(T, V[:m], -cf.T, beta=1.0)
+    G = gram(T, T).cpu().numpy()
+    G = 0.5 * (G + G.T)
+    acc = []
+    for i in range(k):
+        c = np.zeros(k)
+        c[i] = 1.0
+        for _ in range(2):
+            for a in acc:
+                c = c - float(a @ G @ c) * a
+        nrm2 = float(c @ G @ c)
+        if nrm2 > lindep:
+            acc.append(c / np.sqrt(nrm2))
+    if not acc:
+        return []
+    C = np.array(acc)
+    Q = V[m:m + len(acc)]
+    combine(Q, T, C)
+    Gq = gram(Q, Q).cpu().numpy()
+    if np.abs(Gq - np.eye(len(acc))).max() > 1e-8:
+        return _orthonormalise_per_vector(V, m, new, lindep)
+    return list(range(m, m + len(acc)))
+
+
 def davidson(aop, x0, precond, tol=1e-10, max_cycle=100, max_space=12, lindep=1e-14, nroots=1,
              follow_state=True, tol_residual=None, verbose=0, log=None, stats=None):
     """aop(X) maps a device (k, n) block to (k, n).  x0: device (m, n) or a
@@ -118,18 +174,7 @@ def davidson(aop, x0, precond, tol=1e-10, max_cycle=100, max_space=12, lindep=1e
     for icyc in range(max_cycle):
         if stats is not None:
             stats["niter"] = icyc + 1
-        # orthonormalise the new block against V and among itself
-        added = []
-        for i in range(new.shape[0]):
-            t = new[i:i + 1].clone()
-            for _ in range(2):
-                if m + len(added):
-                    cf = gram(V[:m + len(added)], t).cpu().numpy().T
-                    combine(t, V[:m + len(added)], -cf, beta=1.0)
-            nrm2 = float(gram(t, t).cpu().numpy()[0, 0])
-            if nrm2 > lindep:
-                V[m + len(added)].copy_(t[0] / np.sqrt(nrm2))
-                added.append(m + len(added))
+        added = _orthonormalise_into(V, m, new, lindep)
         if not added:
             break
         k0 = m

@@ -335,16 +335,24 @@ def test_kernel_energies(golden_case):
             assert abs(m - sm) < 1e-6
 
 
-def test_kernel_c1_three_roots():
+@pytest.mark.parametrize("device_resident", [False, True])
+def test_kernel_c1_three_roots(device_resident):
+    """C1 (norb 12 (6,6), 3 roots) against the reference's own solver:
+    energies within 1e-9 Eh on both paths.  The host-driven Davidson (the
+    reference's p-space Olsen preconditioner) gives the reference's root-0
+    1-RDM within 1e-8; the device-resident one (diagonal Olsen
+    preconditioner, another iteration path to the same conv_tol, residual
+    1e-5) within 1e-7, the spread of two vectors converged to that residual."""
     P, _, _ = _mods()
     g = load_golden("c1_norb12_6e6e_s0")
     h1, eri = seeded_integrals(12, 24)
     sol = P.csf_solver(None, smult=1)
     sol.nroots = 3
+    sol.device_resident = device_resident
     e, ci = sol.kernel(h1, eri, 12, (6, 6))
     np.testing.assert_allclose(e, g["energies"], atol=1e-9)
     dm1, dm2 = sol.make_rdm12(ci[0], 12, (6, 6))
-    np.testing.assert_allclose(dm1, g["rdm1_root0"], atol=1e-8)
+    np.testing.assert_allclose(dm1, g["rdm1_root0"], atol=1e-7 if device_resident else 1e-8)
     fp = float(np.dot(np.cos(np.arange(dm2.size)), dm2.ravel()))
     assert abs(fp - float(g["fp_rdm2_root0"])) < 1e-6
 
@@ -520,3 +528,26 @@ def test_sigma_plan_c_abi(norb, nelec, smult):
                 assert st == _capi.CSFFCI_ERR_INVALID
         finally:
             lib.csffci_sigma_plan_destroy(plan)
+
+
+@pytest.mark.parametrize("nx,ny,n", [(48, 1, 1000003), (40, 4, 300001), (3, 40, 200003), (64, 4, 70001),
+                                     (1, 1, 17), (2, 3, 5000), (7, 9, 100000), (33, 2, 65536)])
+def test_gram_and_combine_vs_torch(nx, ny, n):
+    """csffci_gram (the skinny kernel for up to 4 vectors on one side, the
+    tiled split-K kernel otherwise) and csffci_combine against a plain torch
+    fp64 reference (x y^T and beta*y + coef x) at 1e-12 relative; the Gram
+    is bit-reproducible from one call to the next."""
+    from pyscf_forge_b200.fci.davidson import combine, gram
+    g = torch.Generator(device="cpu").manual_seed(nx * 1000 + ny)
+    x = torch.randn(nx, n, generator=g, dtype=torch.float64).cuda()
+    y = torch.randn(ny, n, generator=g, dtype=torch.float64).cuda()
+    ref = x @ y.T
+    got = gram(x, y)
+    scale = float(ref.abs().max()) + 1.0
+    assert float((got - ref).abs().max()) < 1e-12 * scale * max(1.0, n / 1e4)
+    assert torch.equal(got, gram(x, y))
+    coef = np.random.default_rng(nx + ny).normal(size=(ny, nx))
+    y0 = y.clone()
+    combine(y, x, coef, beta=0.5)
+    ref2 = 0.5 * y0 + torch.as_tensor(coef, device="cuda") @ x
+    assert float((y - ref2).abs().max()) < 1e-12 * (float(ref2.abs().max()) + 1.0) * max(1.0, nx / 8)
