@@ -354,7 +354,7 @@ def test_kernel_c1_three_roots(device_resident):
     dm1, dm2 = sol.make_rdm12(ci[0], 12, (6, 6))
     np.testing.assert_allclose(dm1, g["rdm1_root0"], atol=1e-7 if device_resident else 1e-8)
     fp = float(np.dot(np.cos(np.arange(dm2.size)), dm2.ravel()))
-    assert abs(fp - float(g["fp_rdm2_root0"])) < 1e-6
+    assert abs(fp - float(g["fp_rdm2_root0"])) < (1e-5 if device_resident else 1e-6)
 
 
 def test_errors_are_raised():
@@ -439,7 +439,8 @@ def test_solver_contract_2e_out_buffers():
 def test_warp_specialised_sigma(norb, nelec, rank, monkeypatch):
     """The warp-specialised sigma kernels (tile variant 4 from 13 orbitals,
     variant 5 -- registers re-split between the roles -- and variant 6 --
-    the same with the alpha rows moved by the bulk-copy engine -- at 16;
+    the same with the alpha rows moved by the bulk-copy engine, and variant
+    7 -- with the alpha scatter on the tail warps -- at 16;
     variant 6 also from a vector 8 bytes off 16-byte alignment, which it
     copies element by element instead): against the
     reference C (1e-10) and against the phase-serial kernel (1e-12), in the
@@ -457,7 +458,7 @@ def test_warp_specialised_sigma(norb, nelec, rank, monkeypatch):
     cases = [(c0, (None,))]
     if na == nb:
         cases = [(c0 + c0.T, (None, 1)), (c0 - c0.T, (-1,))]
-    variants = (4, 5, 6) if norb == 16 else (4,)
+    variants = (4, 5, 6, 7) if norb == 16 else (4,)
     for c, etas in cases:
         c = c / np.linalg.norm(c)
         ref = gasref.contract_2e(h2e_np, c, norb, nelec).ravel()
