@@ -533,7 +533,8 @@ class FCISolver(CSFFCISolver, FCIBase):
                                max_cycle=kwargs.get('max_cycle', self.max_cycle),
                                max_space=kwargs.get('max_space', self.max_space), level_shift=self.level_shift,
                                pspace_size=kwargs.get('pspace_size', self.pspace_size),
-                               conv_tol_residual=getattr(self, 'conv_tol_residual', None))
+                               conv_tol_residual=getattr(self, 'conv_tol_residual', None),
+                               autotune=False)  # the defaults are the single-problem shapes
         p = Problem(norb, _unpack_nelec(nelec, self.spin), self.smult, nroots, h1e, eri)
         e, cis, _, conv = sol.kernel([p], with_rdm=False)[0]
         self.converged = conv if nroots == 1 else [conv] * nroots
