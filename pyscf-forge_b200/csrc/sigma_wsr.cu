@@ -75,8 +75,10 @@ __device__ __forceinline__ void wsr_reg_dec() {
 
 // KS k-steps of 4 (KS = 34 at 16 orbitals), KH = KS/2 per tail K half.
 // TS: the alpha scatter runs on the tail warps, from V in shared memory,
-// instead of on every MMA warp from its accumulators.
-template <int KS, bool TS>
+// instead of on every MMA warp from its accumulators.  CO: the big warps'
+// alpha scatter exchanges values within each quad so that its atomics are
+// sector-coalesced.
+template <int KS, bool TS, bool CO>
 __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
   static_assert(KS % 2 == 0, "the tail warps split K in two equal halves");
   constexpr int NB = WS_NB;
@@ -181,6 +183,36 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
           // the transpose)
           double* const obase = sjob.sym ? sjob.scratch : sjob.sigma;
           const int alim = (int)(sjob.sym ? srow.ja : sjob.Nb);
+          if (CO) {
+            // the four lanes of a quad hold one pair row; exchange values
+            // within the quad so that atomic q of a lane is column 4q+tq:
+            // every instruction then covers 4 consecutive doubles (one
+            // 32-byte sector) per row instead of two sectors
+            const int qbase = lane & ~3, sub = tq >> 1, odd = tq & 1;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int r = h ? r1 : r0;
+              const long long aoff = r < npair ? S.apoff[r] : -1;
+              const unsigned aneg = r < npair ? S.pneg[srow.pc + r] : 0u;
+              double v[4];
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                const int src = qbase + sub + 2 * (q & 1);
+                const double a = __shfl_sync(0xffffffffu, acc[q >> 1][2 * h], src);
+                const double b = __shfl_sync(0xffffffffu, acc[q >> 1][2 * h + 1], src);
+                v[q] = odd ? b : a;
+              }
+              if (aoff >= 0) {
+                double* const abase = obase + aoff;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                  const int J = c * NB + 4 * q + tq;
+                  if (J < alim) atomicAdd(abase + J, rr_flip(v[q], aneg));
+                }
+              }
+            }
+            continue;
+          }
           const int J = c * NB + 2 * tq;
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
@@ -311,7 +343,8 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
 bool sigma_wsr_supported(int norb) { return norb == 16; }
 
 int sigma_wsr_launch(int norb, const csffci_sigma_job_t& job0, long long total_units, long long max_nb,
-                     int max_nla, int max_nlb, cudaStream_t stream, bool bulk, bool tail_scatter) {
+                     int max_nla, int max_nlb, cudaStream_t stream, bool bulk, bool tail_scatter,
+                     bool coalesced) {
   if (!sigma_wsr_supported(norb)) {
     set_error("sigma: the register-split warp-specialised variant covers norb 16, not %d", norb);
     return CSFFCI_ERR_INVALID;
@@ -336,7 +369,8 @@ int sigma_wsr_launch(int norb, const csffci_sigma_job_t& job0, long long total_u
   }
   g.off_extra = extra;
   g.bulk = bulk && ws_bulk_ok(job0) ? 1 : 0;
-  auto kern = tail_scatter ? k_sigma_wsr<KS, true> : k_sigma_wsr<KS, false>;
+  auto kern = tail_scatter ? k_sigma_wsr<KS, true, false>
+                           : coalesced ? k_sigma_wsr<KS, false, true> : k_sigma_wsr<KS, false, false>;
   // setmaxnreg re-splits the registers the launch allocated (128 per
   // thread); with any other count the raise of warpgroups 0-1 could not be
   // met, so refuse rather than launch
@@ -359,7 +393,8 @@ int sigma_wsr_launch(int norb, const csffci_sigma_job_t& job0, long long total_u
   long long grid = nsm;
   if (grid > g.total_units) grid = g.total_units;
   if (grid < 1) return CSFFCI_OK;
-  ProfScope ps(g.bulk ? "k_sigma_wsr_bulk" : tail_scatter ? "k_sigma_wsr_ts" : "k_sigma_wsr", stream);
+  ProfScope ps(g.bulk ? "k_sigma_wsr_bulk" : tail_scatter ? "k_sigma_wsr_ts" : coalesced ? "k_sigma_wsr_co" : "k_sigma_wsr",
+               stream);
   kern<<<(int)grid, WSR_NTH, smem, stream>>>(g);
   return check_launch("sigma (register-split warp-specialised)");
 }
