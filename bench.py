@@ -361,6 +361,8 @@ def run_ours(args, rank_env):
         line["batched"] = run_batched(args.batch)
     if rank == 0 and world == 1 and not args.no_c4:
         line["c4"] = run_c4(ref_check=not args.no_cpu_baseline)
+    if rank == 0 and world == 1 and not args.no_rdm:
+        line["transforms"] = run_transforms()
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -403,6 +405,42 @@ def run_rdm(dmma_peak, cases=None):
     out["note"] = ("adjoint = transition-density / RDM kernel: T slabs <J|E_pq|c> built in shared memory, "
                    "Gram on FP64 DMMA (bra == ket: symmetric half), 1-RDM from the Gram; flops counted "
                    "as the dense 2*ndet*norb^4")
+    return out
+
+
+def run_transforms(workload="cas16", nvecs=(1, 4), reps=5):
+    """The det<->CSF transforms (csffci_det2csf / csffci_csf2det: per npair
+    block a GEMM with the csd_mask gather or scatter fused into it) on the
+    singlet space of a workload, device-timed, with the fraction of the HBM
+    roofline on the compulsory bytes 8*(ndet+ncsf) + 4*ndet per vector."""
+    import torch
+    from pyscf_forge_b200 import _capi
+    from pyscf_forge_b200.csf_fci.csfstring import CSFTransformer
+    norb, nelec, _ = WORKLOADS[workload]
+    t = CSFTransformer(norb, nelec[0], nelec[1], 1)
+    hbm, src = peaks()
+    out = {"workload": "%s singlet (ndet %d, ncsf %d)" % (workload, t.ndet, t.ncsf)}
+    for nv in nvecs:
+        g = torch.Generator(device="cpu").manual_seed(7)
+        x = torch.randn(nv, t.ncsf, generator=g, dtype=torch.float64).cuda()
+        d = t.dev_csf2det(x)
+        torch.cuda.synchronize()
+        for name, fn, arg in (("csf2det", t.dev_csf2det, x), ("det2csf", t.dev_det2csf, d)):
+            fn(arg)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                fn(arg)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            byts = nv * (8.0 * (t.ndet + t.ncsf) + 4.0 * t.ndet)
+            out["%s_nvec%d" % (name, nv)] = {"ms": ms, "GBps": byts / (ms * 1e-3) / 1e9,
+                                             "frac_hbm": byts / (ms * 1e-3) / 1e9 / hbm}
+        del x, d
+    out["peak_note"] = "hbm_gbs %s" % src
     return out
 
 
@@ -573,6 +611,8 @@ def main():
     ap.add_argument("--no-c4", action="store_true", help="skip the CAS(16,16) 4-root solve + RDM backward")
     ap.add_argument("--c4-only", action="store_true", help="only the CAS(16,16) 4-root solve + RDM backward")
     ap.add_argument("--c4-max-cycle", type=int, default=None, help="Davidson iterations of the C4 solve")
+    ap.add_argument("--transforms-only", action="store_true",
+                    help="only the det<->CSF transform timing of --workload (profiling captures)")
     ap.add_argument("--rdm-only", default="", help="only the RDM timing of these cases "
                     "(cas16_singlet_1root,cas14_sa2), for profiling captures")
     ap.add_argument("--batch", type=int, default=128, help="problems in the batched-solves measurement")
@@ -584,6 +624,12 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
         run_reference(args, (rank, world))
+        return
+    if args.transforms_only:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        if rank == 0:
+            print(json.dumps(run_transforms(args.workload)), flush=True)
         return
     if args.c4_only:
         import torch

@@ -58,9 +58,7 @@ int sigma_rr_single_variant(int norb) {
   if (env) {
     const int v = atoi(env);
     if (v == RR_VARIANT_WS && sigma_ws_supported(norb)) return RR_VARIANT_WS;
-    if ((v == RR_VARIANT_WSR || v == RR_VARIANT_WSR_BULK || v == RR_VARIANT_WSR_TS || v == RR_VARIANT_WSR_CO) &&
-        sigma_wsr_supported(norb))
-      return v;
+    if ((v == RR_VARIANT_WSR || v == RR_VARIANT_WSR_BULK) && sigma_wsr_supported(norb)) return v;
     if (rr_variant_valid(norb, v)) return v;
   }
   // measured on B200 (singlet, one problem): 14 orbitals 7.61 -> 6.31 ms,
@@ -120,15 +118,13 @@ int sigma_rr_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev,
     }
     return sigma_ws_launch(norb, job0, total_units, max_nb, max_nla, max_nlb, stream);
   }
-  if (variant == RR_VARIANT_WSR || variant == RR_VARIANT_WSR_BULK || variant == RR_VARIANT_WSR_TS ||
-      variant == RR_VARIANT_WSR_CO) {
+  if (variant == RR_VARIANT_WSR || variant == RR_VARIANT_WSR_BULK) {
     if (jobs_dev) {
       set_error("sigma: the register-split variant takes one problem, not a job table");
       return CSFFCI_ERR_INVALID;
     }
     return sigma_wsr_launch(norb, job0, total_units, max_nb, max_nla, max_nlb, stream,
-                            variant == RR_VARIANT_WSR_BULK, variant == RR_VARIANT_WSR_TS,
-                            variant == RR_VARIANT_WSR_CO);
+                            variant == RR_VARIANT_WSR_BULK);
   }
   if (!rr_variant_valid(norb, variant)) {
     set_error("sigma: tile variant %d is not available for norb=%d", variant, norb);

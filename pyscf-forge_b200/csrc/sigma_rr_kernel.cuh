@@ -426,14 +426,9 @@ int sigma_ws_launch(int norb, const csffci_sigma_job_t& job0, long long total_un
 constexpr int RR_VARIANT_WSR = 5;
 // the same with the alpha rows moved by the bulk-copy engine
 constexpr int RR_VARIANT_WSR_BULK = 6;
-// the register-split kernel with the alpha scatter on its tail warps
-constexpr int RR_VARIANT_WSR_TS = 7;
-// the register-split kernel with its alpha-scatter atomics sector-coalesced
-constexpr int RR_VARIANT_WSR_CO = 8;
 bool sigma_wsr_supported(int norb);
 int sigma_wsr_launch(int norb, const csffci_sigma_job_t& job0, long long total_units, long long max_nb,
-                     int max_nla, int max_nlb, cudaStream_t stream, bool bulk, bool tail_scatter,
-                     bool coalesced);
+                     int max_nla, int max_nlb, cudaStream_t stream, bool bulk);
 bool rr_variant_valid(int norb, int v);
 int rr_default_variant(int norb);
 int sigma_rr_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev, const csffci_sigma_job_t& job0,

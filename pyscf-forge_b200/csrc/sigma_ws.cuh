@@ -161,11 +161,7 @@ __device__ __forceinline__ bool ws_row_setup(const RRArgs& g, const WSShared& S,
 // together, every load of the pass issued before the dependent ones (a
 // mover is often the only warp of the role on its scheduler, so this
 // instruction-level parallelism is its way to hide latency).
-// TREL > 0: another role (TREL threads besides the movers) also reads V of
-// every tile (the register-split kernel's alpha scatter on its tail warps)
-// and releases the stage on barrier 10+s; the movers wait for that release
-// before refilling the stage, and at the end of a row for its last tiles.
-template <int NTH, int NMOV, int RU, int TREL = 0>
+template <int NTH, int NMOV, int RU>
 __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S, int tid, int warp, int lane,
                                               int mtid, int mwarp) {
   constexpr int NB = WS_NB;
@@ -199,7 +195,6 @@ __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S
           // copies of tile c into stage c % 3 (its last tile, c-3, was
           // scattered at step c-1): alpha rows of c, beta links, zero rows
           const int s = c % WS_STAGES;
-          if (TREL > 0 && c >= WS_STAGES) ws_bar_sync(10 + s, TREL + MTH);  // tile c-3 released
           double* Dd = S.Dbuf + s * dsz;
           csffci_link_t* Ld = S.Lbuf + s * lsz;
           const long long j1 = (long long)c * NB;
@@ -315,8 +310,6 @@ __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S
           }
         }
       }
-      if (TREL > 0)  // releases of the row's last tiles, not waited for above
-        for (int t = max(0, nch - WS_STAGES); t < nch; ++t) ws_bar_sync(10 + t % WS_STAGES, TREL + MTH);
     }
   }
 }

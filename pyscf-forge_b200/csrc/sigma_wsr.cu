@@ -48,20 +48,14 @@ constexpr int WSR_NW = WSR_NBIG + WSR_NTAIL + WSR_NMOV;
 constexpr int WSR_NTH = WSR_NW * 32;
 constexpr int WSR_NMMA = (WSR_NBIG + WSR_NTAIL) * 32;
 constexpr int WSR_REG_LAUNCH = 128;
-constexpr int WSR_TS_BIG = 168, WSR_TS_TAIL = 112, WSR_TS_MOV = 64;
-// per-thread registers of the three roles after the re-split; TS: the
-// alpha scatter on the tail warps (big MMA warps need fewer, tail more)
-template <bool TS>
-struct WsrRegs {
-  static constexpr int BIG = TS ? WSR_TS_BIG : 176;
-  static constexpr int TAIL = TS ? WSR_TS_TAIL : 104;
-  static constexpr int MOV = TS ? WSR_TS_MOV : 56;
-  static_assert(2 * 128 * BIG + 128 * TAIL + 128 * MOV <= WSR_NTH * WSR_REG_LAUNCH,
-                "the re-split registers fit in the launch's allocation");
-  static_assert(BIG % 8 == 0 && TAIL % 8 == 0 && MOV % 8 == 0 && MOV >= 24 && BIG <= 256,
-                "setmaxnreg counts are multiples of 8 in [24, 256]");
-};
+constexpr int WSR_REG_BIG = 176;
+constexpr int WSR_REG_TAIL = 104;
+constexpr int WSR_REG_MOV = 56;
 constexpr int WSR_RU = 3;  // mover links per pass: 8 link rows per pass x 3 = 24 divides 72
+static_assert(2 * 128 * WSR_REG_BIG + 128 * WSR_REG_TAIL + 128 * WSR_REG_MOV <= WSR_NTH * WSR_REG_LAUNCH,
+              "the re-split registers fit in the launch's allocation");
+static_assert(WSR_REG_BIG % 8 == 0 && WSR_REG_TAIL % 8 == 0 && WSR_REG_MOV % 8 == 0 && WSR_REG_MOV >= 24,
+              "setmaxnreg counts are multiples of 8 in [24, 256]");
 static_assert(WSR_NTH * WSR_REG_LAUNCH == 65536, "the launch takes the whole register file");
 
 template <int N>
@@ -73,12 +67,8 @@ __device__ __forceinline__ void wsr_reg_dec() {
   asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(N));
 }
 
-// KS k-steps of 4 (KS = 34 at 16 orbitals), KH = KS/2 per tail K half.
-// TS: the alpha scatter runs on the tail warps, from V in shared memory,
-// instead of on every MMA warp from its accumulators.  CO: the big warps'
-// alpha scatter exchanges values within each quad so that its atomics are
-// sector-coalesced.
-template <int KS, bool TS, bool CO>
+// KS k-steps of 4 (KS = 34 at 16 orbitals), KH = KS/2 per tail K half
+template <int KS>
 __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
   static_assert(KS % 2 == 0, "the tail warps split K in two equal halves");
   constexpr int NB = WS_NB;
@@ -113,7 +103,7 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
 
   if (warp < WSR_NBIG) {
     // ---- big MMA warps: 16 rows each, m16n8k4 ----
-    wsr_reg_inc<WsrRegs<TS>::BIG>();
+    wsr_reg_inc<WSR_REG_BIG>();
     const int gq = lane >> 2, tq = lane & 3;
     const int r0 = 16 * warp + gq, r1 = r0 + 8;
     double a0[KS], a1[KS];
@@ -177,42 +167,11 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
           }
           if (g.bulk) ws_fence_proxy_async();  // V before the stage's next bulk copy
           ws_bar_arrive(4 + s, WSR_NTH);  // V of tile c is written
-          if (TS) continue;
           // alpha scatter of this lane's two pair rows from the accumulators
           // (J < Ja in the spin-symmetric mode, whose column Ja is left to
           // the transpose)
           double* const obase = sjob.sym ? sjob.scratch : sjob.sigma;
           const int alim = (int)(sjob.sym ? srow.ja : sjob.Nb);
-          if (CO) {
-            // the four lanes of a quad hold one pair row; exchange values
-            // within the quad so that atomic q of a lane is column 4q+tq:
-            // every instruction then covers 4 consecutive doubles (one
-            // 32-byte sector) per row instead of two sectors
-            const int qbase = lane & ~3, sub = tq >> 1, odd = tq & 1;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              const int r = h ? r1 : r0;
-              const long long aoff = r < npair ? S.apoff[r] : -1;
-              const unsigned aneg = r < npair ? S.pneg[srow.pc + r] : 0u;
-              double v[4];
-#pragma unroll
-              for (int q = 0; q < 4; ++q) {
-                const int src = qbase + sub + 2 * (q & 1);
-                const double a = __shfl_sync(0xffffffffu, acc[q >> 1][2 * h], src);
-                const double b = __shfl_sync(0xffffffffu, acc[q >> 1][2 * h + 1], src);
-                v[q] = odd ? b : a;
-              }
-              if (aoff >= 0) {
-                double* const abase = obase + aoff;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                  const int J = c * NB + 4 * q + tq;
-                  if (J < alim) atomicAdd(abase + J, rr_flip(v[q], aneg));
-                }
-              }
-            }
-            continue;
-          }
           const int J = c * NB + 2 * tq;
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
@@ -232,7 +191,7 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
     }
   } else if (warp < WSR_NBIG + WSR_NTAIL) {
     // ---- tail MMA warps: rows 128..135, one n-tile and one K half each ----
-    wsr_reg_dec<WsrRegs<TS>::TAIL>();
+    wsr_reg_dec<WSR_REG_TAIL>();
     const int gq = lane >> 2, tq = lane & 3;
     const int tw = warp - WSR_NBIG;
     const int nt = tw & 1, kh = tw >> 1;
@@ -288,32 +247,6 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
             }
           }
           if (g.bulk) ws_fence_proxy_async();
-          if (TS) {
-            // every V row of tile c is written (the big MMA warps arrive,
-            // the tail warps and the movers wait); the tail warps then run
-            // the alpha scatter of all pair rows from shared memory: 16
-            // lanes per pair row, sigma[Ka][J] += sign V[pq][J], coalesced
-            // over J (J < Ja in the spin-symmetric mode), and release the
-            // stage to the movers
-            ws_bar_sync(4 + s, WSR_NTH);
-            const int ttid = tw * 32 + lane;
-            const int col = ttid & (NB - 1), rsub = ttid / NB;
-            const long long J = (long long)c * NB + col;
-            const long long alim = sjob.sym ? srow.ja : sjob.Nb;
-            if (J < alim) {
-              double* const obase = (sjob.sym ? sjob.scratch : sjob.sigma) + J;
-              const double* const Vs = S.Dbuf + s * dsz + col;
-              const int nla = sjob.nla;
-#pragma unroll 1
-              for (int l = rsub; l < nla; l += WSR_NTAIL * 32 / NB) {
-                const RRAlpha a = S.al[l];
-                atomicAdd(obase + a.off, rr_flip(Vs[a.drow], a.neg));
-              }
-            }
-            ws_bar_arrive(10 + s, WSR_NTAIL * 32 + WSR_NMOV * 32);  // stage s released
-            tpar ^= 1;
-            continue;
-          }
           ws_bar_arrive(4 + s, WSR_NTH);  // V of tile c is written
           if (!kh) {
             const long long aoff = rt < npair ? S.apoff[rt] : -1;
@@ -331,20 +264,16 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
       }
     }
   } else {
-    wsr_reg_dec<WsrRegs<TS>::MOV>();
+    wsr_reg_dec<WSR_REG_MOV>();
     const int mw = warp - WSR_NBIG - WSR_NTAIL;
-    if (TS)
-      ws_mover_role<WSR_NTH, WSR_NMOV, WSR_RU, WSR_NTAIL * 32>(g, S, tid, warp, lane, mw * 32 + lane, mw);
-    else
-      ws_mover_role<WSR_NTH, WSR_NMOV, WSR_RU>(g, S, tid, warp, lane, mw * 32 + lane, mw);
+    ws_mover_role<WSR_NTH, WSR_NMOV, WSR_RU>(g, S, tid, warp, lane, mw * 32 + lane, mw);
   }
 }
 
 bool sigma_wsr_supported(int norb) { return norb == 16; }
 
 int sigma_wsr_launch(int norb, const csffci_sigma_job_t& job0, long long total_units, long long max_nb,
-                     int max_nla, int max_nlb, cudaStream_t stream, bool bulk, bool tail_scatter,
-                     bool coalesced) {
+                     int max_nla, int max_nlb, cudaStream_t stream, bool bulk) {
   if (!sigma_wsr_supported(norb)) {
     set_error("sigma: the register-split warp-specialised variant covers norb 16, not %d", norb);
     return CSFFCI_ERR_INVALID;
@@ -369,8 +298,7 @@ int sigma_wsr_launch(int norb, const csffci_sigma_job_t& job0, long long total_u
   }
   g.off_extra = extra;
   g.bulk = bulk && ws_bulk_ok(job0) ? 1 : 0;
-  auto kern = tail_scatter ? k_sigma_wsr<KS, true, false>
-                           : coalesced ? k_sigma_wsr<KS, false, true> : k_sigma_wsr<KS, false, false>;
+  auto kern = k_sigma_wsr<KS>;
   // setmaxnreg re-splits the registers the launch allocated (128 per
   // thread); with any other count the raise of warpgroups 0-1 could not be
   // met, so refuse rather than launch
@@ -393,8 +321,7 @@ int sigma_wsr_launch(int norb, const csffci_sigma_job_t& job0, long long total_u
   long long grid = nsm;
   if (grid > g.total_units) grid = g.total_units;
   if (grid < 1) return CSFFCI_OK;
-  ProfScope ps(g.bulk ? "k_sigma_wsr_bulk" : tail_scatter ? "k_sigma_wsr_ts" : coalesced ? "k_sigma_wsr_co" : "k_sigma_wsr",
-               stream);
+  ProfScope ps(g.bulk ? "k_sigma_wsr_bulk" : "k_sigma_wsr", stream);
   kern<<<(int)grid, WSR_NTH, smem, stream>>>(g);
   return check_launch("sigma (register-split warp-specialised)");
 }

@@ -439,9 +439,7 @@ def test_solver_contract_2e_out_buffers():
 def test_warp_specialised_sigma(norb, nelec, rank, monkeypatch):
     """The warp-specialised sigma kernels (tile variant 4 from 13 orbitals,
     variant 5 -- registers re-split between the roles -- and variant 6 --
-    the same with the alpha rows moved by the bulk-copy engine, variant 7
-    -- with the alpha scatter on the tail warps -- and variant 8 -- with
-    sector-coalesced alpha-scatter atomics -- at 16;
+    the same with the alpha rows moved by the bulk-copy engine -- at 16;
     variant 6 also from a vector 8 bytes off 16-byte alignment, which it
     copies element by element instead): against the
     reference C (1e-10) and against the phase-serial kernel (1e-12), in the
@@ -459,7 +457,7 @@ def test_warp_specialised_sigma(norb, nelec, rank, monkeypatch):
     cases = [(c0, (None,))]
     if na == nb:
         cases = [(c0 + c0.T, (None, 1)), (c0 - c0.T, (-1,))]
-    variants = (4, 5, 6, 7, 8) if norb == 16 else (4,)
+    variants = (4, 5, 6) if norb == 16 else (4,)
     for c, etas in cases:
         c = c / np.linalg.norm(c)
         ref = gasref.contract_2e(h2e_np, c, norb, nelec).ravel()
