@@ -555,13 +555,18 @@ def run_batched(nprob):
     Bt.BatchedCSFSolver(**kw).kernel(probs)  # warm-up: transformers, autotuner
     Bt.solve_plain(probs[:8], **kw)
     torch.cuda.synchronize()
+    from pyscf_forge_b200 import _capi
     sol = Bt.BatchedCSFSolver(**kw)
+    _capi.profile_enable(True)
     t0 = time.perf_counter()
     rb = sol.kernel(probs)
     torch.cuda.synchronize()
     tb = time.perf_counter() - t0
+    prof = _capi.profile_report()
+    _capi.profile_enable(False)
+    plain_phases = {}
     t0 = time.perf_counter()
-    rp = Bt.solve_plain(probs, **kw)
+    rp = Bt.solve_plain(probs, phases=plain_phases, **kw)
     torch.cuda.synchronize()
     tp = time.perf_counter() - t0
     de = max(float(np.max(np.abs(a[0] - b[0]))) for a, b in zip(rb, rp))
@@ -585,7 +590,10 @@ def run_batched(nprob):
     return {"metric": "batched solves+RDMs/s", "value": nprob / tb, "unit": "solves/s",
             "plain_value": nprob / tp, "speedup_vs_plain": tp / tb, "seconds": tb, "plain_seconds": tp,
             "problems": nprob, "roots": nroots, "converged_problems": int(sum(bool(a[3]) for a in rb)),
-            "iterations": sol.iterations, "max_abs_dE_vs_plain": de,
+            "iterations": sol.iterations, "phase_s": {k: round(v, 4) for k, v in sol.phase_s.items()},
+            "plain_phase_s": {k: round(v, 4) for k, v in plain_phases.items()},
+            "kernel_ms": {k: round(v[1], 2) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])[:12]},
+            "max_abs_dE_vs_plain": de,
             "max_abs_dE_vs_plain_converged": de_conv,
             "tile_variants": {str(k): v for k, v in (sol.tile_variants or {}).items()},
             **ref,

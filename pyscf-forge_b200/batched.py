@@ -18,6 +18,7 @@ seeded uneven batch of the benchmark configuration.
 No counterpart in the reference, which solves one problem per call.
 """
 import ctypes
+import time
 from math import comb
 
 import numpy as np
@@ -81,17 +82,25 @@ def make_uneven_batch(nprob=128, seed0=1000, norb_lo=6, norb_hi=12):
     return out
 
 
-def solve_plain(problems, with_rdm=True, **solver_attrs):
-    """One problem at a time through the public FCISolver API."""
+def solve_plain(problems, with_rdm=True, phases=None, **solver_attrs):
+    """One problem at a time through the public FCISolver API.  phases (a
+    dict, optional) accumulates the wall time of the solver's phases and of
+    the RDMs."""
     out = []
     for p in problems:
         sol = FCISolver(None, smult=p.smult)
         sol.nroots = p.nroots
         for k, v in solver_attrs.items():
             setattr(sol, k, v)
+        t0 = time.perf_counter()
         e, ci = sol.kernel(p.h1, p.eri, p.norb, p.nelec)
+        t1 = time.perf_counter()
         cis = ci if isinstance(ci, list) else [ci]
         rdms = [sol.make_rdm12(c, p.norb, p.nelec) for c in cis] if with_rdm else None
+        if phases is not None:
+            for k, v in getattr(sol, "phase_s", {"kernel": t1 - t0}).items():
+                phases[k] = phases.get(k, 0.0) + v
+            phases["rdm"] = phases.get("rdm", 0.0) + time.perf_counter() - t1
         out.append((np.atleast_1d(e), cis, rdms))
     return out
 
@@ -288,8 +297,18 @@ class BatchedCSFSolver:
         return _transform_jobs(S.t, src, ld_src, dst, ld_dst, nvec)
 
     # ---- solve -------------------------------------------------------------
+    def _mark(self, name):
+        """Wall time of the phase that just ended (device synchronised)."""
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        self.phase_s[name] = self.phase_s.get(name, 0.0) + t - self._t
+        self._t = t
+
     def kernel(self, problems, with_rdm=True):
         dev = device()
+        self.phase_s = {}
+        torch.cuda.synchronize()
+        self._t = time.perf_counter()
         states = []
         exact = []
         for ip, p in enumerate(problems):
@@ -315,6 +334,7 @@ class BatchedCSFSolver:
                 exact.append(S)
             else:
                 states.append(S)
+        self._mark("setup")
         for S in exact:
             addr, h0 = csf_pspace(None, S.p.h1, S.p.eri, S.norb, S.nelec, S.t, hdiag_det=S.hd,
                                   hdiag_csf=S.hc, npsp=S.n)
@@ -325,13 +345,17 @@ class BatchedCSFSolver:
             S.e = w[:S.k]
             S.conv = [True] * S.k
         if self.engine == "device":
+            self._mark("exact_pspace")
             self._device_davidson(states)
+            self._mark("davidson")
         elif self.engine == "host":
             self._davidson(states)
         else:
             raise ValueError("engine must be 'device' or 'host'")
         allS = sorted(exact + states, key=lambda s: s.ip)
-        return self._finish(allS, with_rdm)
+        out = self._finish(allS, with_rdm)
+        self._mark("finish_rdm")
+        return out
 
     def _device_davidson(self, states):
         """All problems through one csffci_batch plan: tables built once,

@@ -537,6 +537,7 @@ class FCISolver(CSFFCISolver, FCIBase):
                                autotune=False)  # the defaults are the single-problem shapes
         p = Problem(norb, _unpack_nelec(nelec, self.spin), self.smult, nroots, h1e, eri)
         e, cis, _, conv = sol.kernel([p], with_rdm=False)[0]
+        self.phase_s = dict(sol.phase_s)
         self.converged = conv if nroots == 1 else [conv] * nroots
         self.niter = int(sol.niter[0]) if sol.niter is not None else 0
         if nroots > 1:
