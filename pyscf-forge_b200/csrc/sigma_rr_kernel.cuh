@@ -33,6 +33,7 @@ struct RRArgs {
   unsigned off_extra;  // register-split kernel: tail partial sums
   unsigned off_mbar;   // warp-specialised kernels: one mbarrier per stage
   int bulk;            // warp-specialised kernels: alpha rows by bulk copy
+  int parts;           // warp-specialised kernels: parts per row unit (tile ranges)
 };
 
 // Alpha link of the current row Ja as the tile loops use it: the offset
@@ -52,7 +53,8 @@ __device__ __forceinline__ double rr_flip(double x, unsigned mask) {
 // state of the row Ja a CTA is working on (uniform over the CTA)
 struct RRRow {
   long long ja, jend;
-  int nchunk, nzero, pc, pad;
+  int nchunk, nzero, pc;
+  int c0;  // warp-specialised kernels: first tile of the row's part
 };
 
 // link entry as two words: addr, then op | sign << 16 | pair << 24 (the

@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(WSLayout<MT>::NTOT * 32, 1) k_sigma_ws(RRArgs 
             double* const abase = (sjob.sym ? sjob.scratch : sjob.sigma) + aoff;
             const unsigned aneg = S.pneg[srow.pc + r0];
             const int alim = (int)(sjob.sym ? srow.ja : sjob.Nb);
-            const int J = c * NB + 8 * t0 + 2 * tq;
+            const int J = (srow.c0 + c) * NB + 8 * t0 + 2 * tq;
             if (J < alim) atomicAdd(abase + J, rr_flip(acc[0][0], aneg));
             if (J + 1 < alim) atomicAdd(abase + J + 1, rr_flip(acc[0][1], aneg));
             if (!part) {
@@ -242,7 +242,11 @@ int sigma_ws_launch(int norb, const csffci_sigma_job_t& job0, long long total_un
   g.jobs = nullptr;
   g.job0 = job0;
   g.njobs = 1;
-  g.total_units = total_units;
+  // spin-symmetric row units (pairs of rows of equal total length) are cut
+  // in two tile ranges: 2 x (Na+1)/2 units balance the 148 SMs to within a
+  // fraction of a unit
+  g.parts = job0.sym ? 2 : 1;
+  g.total_units = total_units * g.parts;
   const size_t smem = ws_layout(g, npair, 8, max_nb, max_nla, max_nlb, 0, nullptr);
   if (smem == 0) {
     set_error("sigma: warp-specialised tiles exceed shared memory (norb %d)", norb);

@@ -98,13 +98,17 @@ struct WSShared {
 // same arguments, and it synchronises the CTA on barrier 9): the alpha links
 // of row Ja, the rows without one, the sign masks of this row (in half par
 // of pneg) and the copy of c row Ja.  Returns false (for every thread) when
-// the spin-symmetric unit has no second row.
+// the spin-symmetric unit has no second row.  A unit (index iu) is part
+// iu % g.parts of row unit iu / g.parts: the tiles [c0, c0 + nchunk) of the
+// row, so that units are small enough to balance the SMs.
 template <int NTH, int NB>
-__device__ __forceinline__ bool ws_row_setup(const RRArgs& g, const WSShared& S, long long lu, int w, int par,
+__device__ __forceinline__ bool ws_row_setup(const RRArgs& g, const WSShared& S, long long iu, int w, int par,
                                              int tid, int warp, int lane) {
   const csffci_sigma_job_t& sjob = g.job0;
   const long long Nb = sjob.Nb;
   const int nla = sjob.nla, npair = g.npair, ds = g.ds;
+  const long long lu = iu / g.parts;
+  const int part = (int)(iu - lu * g.parts);
   long long ja = lu;
   if (sjob.sym && w == 1) {
     ja = sjob.Na - 1 - lu;
@@ -115,7 +119,9 @@ __device__ __forceinline__ bool ws_row_setup(const RRArgs& g, const WSShared& S,
   if (tid == 0) {
     S.srow->ja = ja;
     S.srow->jend = sjob.sym ? ja + 1 : Nb;
-    S.srow->nchunk = (int)((S.srow->jend + NB - 1) / NB);
+    const int nt = (int)((S.srow->jend + NB - 1) / NB);
+    S.srow->c0 = (int)((long long)part * nt / g.parts);
+    S.srow->nchunk = (int)((long long)(part + 1) * nt / g.parts) - S.srow->c0;
     S.srow->pc = par * npair;
   }
   for (int r = tid; r < npair; r += NTH) {
@@ -181,7 +187,7 @@ __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S
       cp_async_wait_all();
       ws_bar_sync(9, NTH);
       const RRRow& srow = *S.srow;
-      const int nch = srow.nchunk;
+      const int nch = srow.nchunk, c0 = srow.c0;  // local tiles c, global tiles c0 + c
       const long long jend = srow.jend, ja = srow.ja, Nb = sjob.Nb;
       const int nla = sjob.nla, nlb = sjob.nlb, nz = srow.nzero;
       const unsigned* pc = S.pneg + srow.pc;
@@ -197,7 +203,7 @@ __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S
           const int s = c % WS_STAGES;
           double* Dd = S.Dbuf + s * dsz;
           csffci_link_t* Ld = S.Lbuf + s * lsz;
-          const long long j1 = (long long)c * NB;
+          const long long j1 = (long long)(c0 + c) * NB;
           const int nc = (int)min((long long)NB, jend - j1);
           if (g.bulk) {
             // one mover warp hands the alpha rows of tile c to the bulk-copy
@@ -257,7 +263,7 @@ __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S
           ws_bar_sync(7, MTH);
           double* D = S.Dbuf + s * dsz;
           const csffci_link_t* Lt = S.Lbuf + s * lsz;
-          const int ncol = (int)min((long long)NB, jend - (long long)(c - 1) * NB);
+          const int ncol = (int)min((long long)NB, jend - (long long)(c0 + c - 1) * NB);
           if (jl < ncol)
             for (int m0 = ml; m0 < nlb; m0 += RU * MPASS) {
               // distinct links of a column have distinct pairs, so the
@@ -289,7 +295,7 @@ __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S
           ws_bar_sync(4 + s, NTH);  // V of tile c-2 is written
           const double* D = S.Dbuf + s * dsz;
           const csffci_link_t* Lt = S.Lbuf + s * lsz;
-          const long long j0 = (long long)(c - 2) * NB;
+          const long long j0 = (long long)(c0 + c - 2) * NB;
           const int ncol = (int)min((long long)NB, jend - j0);
           if (jl < ncol) {
             double* const orow = out + ja * Nb;

@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
           // the transpose)
           double* const obase = sjob.sym ? sjob.scratch : sjob.sigma;
           const int alim = (int)(sjob.sym ? srow.ja : sjob.Nb);
-          const int J = c * NB + 2 * tq;
+          const int J = (srow.c0 + c) * NB + 2 * tq;
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             const int r = h ? r1 : r0;
@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
               double* const abase = (sjob.sym ? sjob.scratch : sjob.sigma) + aoff;
               const unsigned aneg = S.pneg[srow.pc + rt];
               const int alim = (int)(sjob.sym ? srow.ja : sjob.Nb);
-              const int J = c * NB + 8 * nt + 2 * tq;
+              const int J = (srow.c0 + c) * NB + 8 * nt + 2 * tq;
               if (J < alim) atomicAdd(abase + J, rr_flip(acc0, aneg));
               if (J + 1 < alim) atomicAdd(abase + J + 1, rr_flip(acc1, aneg));
             }
@@ -289,7 +289,8 @@ int sigma_wsr_launch(int norb, const csffci_sigma_job_t& job0, long long total_u
   g.jobs = nullptr;
   g.job0 = job0;
   g.njobs = 1;
-  g.total_units = total_units;
+  g.parts = job0.sym ? 2 : 1;  // as in sigma_ws_launch
+  g.total_units = total_units * g.parts;
   unsigned extra = 0;
   const size_t smem = ws_layout(g, npair, 8, max_nb, max_nla, max_nlb, 4 * 64 * sizeof(double), &extra);
   if (smem == 0) {

@@ -119,6 +119,105 @@ __global__ void __launch_bounds__(256) k_block_gemm(BlockGemmArgs g) {
   }
 }
 
+// Blocks with few determinants and CSFs per configuration (at CAS(16,16)
+// the npair >= 3 blocks: at most 252 determinants and 42 CSFs, 98 % of the
+// configurations and 70 % of the determinants) make poor 64x64 GEMM tiles:
+// N = ncsf and K = ndet are far below the tile, so most of the tile's work
+// is padding.  Here one thread takes one (vector, configuration): the
+// block's umat sits in shared memory (every thread of a warp reads the same
+// element, a broadcast), and the configuration's gathered determinant
+// values (det->CSF) or its CSF coefficients (CSF->det) meet it in
+// registers.  The sums run over the determinants (det->CSF) or the CSFs
+// (CSF->det) in ascending order with the same fused multiply-adds as the
+// GEMM path, so both give the same bits.
+constexpr int SMALL_MAX_NCSF = 48;
+constexpr size_t SMALL_MAX_UMAT_BYTES = 96 * 1024;
+
+template <int MODE, int NC>
+__global__ void __launch_bounds__(256) k_block_small(BlockGemmArgs g) {
+  extern __shared__ double Us[];  // umat [ndet][ncsf]
+  const int nd = g.ndet, nc = g.ncsf;
+  for (int i = threadIdx.x; i < nd * nc; i += blockDim.x) Us[i] = g.umat[i];
+  __syncthreads();
+  const int64_t M = (int64_t)g.nvec * g.nconf;
+  for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < M;
+       m += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t vec = m / g.nconf, conf = m - vec * g.nconf;
+    const int64_t cf = g.conf_sel ? g.conf_sel[conf] : conf;
+    const uint32_t* mk = g.mask + g.csd_off + cf * nd;
+    if (MODE == MODE_DET2CSF) {
+      double acc[NC];
+#pragma unroll
+      for (int k = 0; k < NC; ++k) acc[k] = 0.0;
+      const double* xv = g.x + vec * g.ldx;
+      for (int x = 0; x < nd; ++x) {
+        const double v = xv[mk[x]];
+        const double* u = Us + x * nc;
+#pragma unroll
+        for (int k = 0; k < NC; ++k)
+          if (k < nc) acc[k] = fma(v, u[k], acc[k]);
+      }
+      double* yo = g.y + vec * g.ldy + g.csf_off + conf * nc;
+#pragma unroll
+      for (int k = 0; k < NC; ++k)
+        if (k < nc) yo[k] = g.sign * acc[k];
+    } else {
+      double cin[NC];
+      const double* xi = g.x + vec * g.ldx + g.csf_off + conf * nc;
+#pragma unroll
+      for (int k = 0; k < NC; ++k) cin[k] = k < nc ? xi[k] : 0.0;
+      double* yv = g.y + vec * g.ldy;
+      for (int x = 0; x < nd; ++x) {
+        const double* u = Us + x * nc;
+        double sacc = 0.0;
+#pragma unroll
+        for (int k = 0; k < NC; ++k)
+          if (k < nc) sacc = fma(cin[k], u[k], sacc);
+        yv[mk[x]] = g.sign * sacc;
+      }
+    }
+  }
+}
+
+// profiler names per npair block (kernel timing by block)
+static const char* block_kernel_name(bool small, int npair) {
+  static const char* sm[9] = {"k_block_small_np0", "k_block_small_np1", "k_block_small_np2", "k_block_small_np3",
+                              "k_block_small_np4", "k_block_small_np5", "k_block_small_np6", "k_block_small_np7",
+                              "k_block_small_np8+"};
+  static const char* gm[9] = {"k_block_gemm_np0", "k_block_gemm_np1", "k_block_gemm_np2", "k_block_gemm_np3",
+                              "k_block_gemm_np4", "k_block_gemm_np5", "k_block_gemm_np6", "k_block_gemm_np7",
+                              "k_block_gemm_np8+"};
+  const int i = npair < 0 ? 0 : npair > 8 ? 8 : npair;
+  return small ? sm[i] : gm[i];
+}
+
+template <int MODE, int NC>
+static int launch_small(const BlockGemmArgs& g, cudaStream_t stream, int npair) {
+  const size_t smem = (size_t)g.ndet * g.ncsf * sizeof(double);
+  auto kern = k_block_small<MODE, NC>;
+  if (smem > 48 * 1024) CSF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int64_t M = (int64_t)g.nvec * g.nconf;
+  {
+    ProfScope ps_(block_kernel_name(true, npair), stream);
+    kern<<<grid_for(M, 256, 148 * 8), 256, smem, stream>>>(g);
+  }
+  return check_launch("det/csf transform (small blocks)");
+}
+
+template <int MODE>
+static int run_small(const BlockGemmArgs& g, cudaStream_t stream, int npair) {
+  if (g.ncsf <= 2) return launch_small<MODE, 2>(g, stream, npair);
+  if (g.ncsf <= 8) return launch_small<MODE, 8>(g, stream, npair);
+  if (g.ncsf <= 16) return launch_small<MODE, 16>(g, stream, npair);
+  if (g.ncsf <= 32) return launch_small<MODE, 32>(g, stream, npair);
+  return launch_small<MODE, SMALL_MAX_NCSF>(g, stream, npair);
+}
+
+static bool small_block(const csffci_block_t& B) {
+  return B.ncsf <= SMALL_MAX_NCSF && (size_t)B.ndet * B.ncsf * sizeof(double) <= SMALL_MAX_UMAT_BYTES &&
+         B.ndet <= 256;
+}
+
 __global__ void k_zero_rows(double* y, int64_t ldy, int nvec, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)nvec * n;
        i += (int64_t)gridDim.x * blockDim.x) {
@@ -150,11 +249,16 @@ static int run_blocks(int nvec, const double* x, int64_t ldx, double* y, int64_t
     g.ncsf = B.ncsf;
     g.nvec = nvec;
     g.sign = B.sign;
+    if (small_block(B)) {
+      const int st = run_small<MODE>(g, stream, B.npair);
+      if (st) return st;
+      continue;
+    }
     int64_t M = (int64_t)nvec * B.nconf;
     int N = (MODE == MODE_DET2CSF) ? B.ncsf : B.ndet;
     int64_t tiles = ((M + TBM - 1) / TBM) * ((N + TBN - 1) / TBN);
     {
-      ProfScope ps_("k_block_gemm", stream);
+      ProfScope ps_(block_kernel_name(false, B.npair), stream);
       k_block_gemm<MODE><<<grid_for(tiles, 1, 148 * 8), 256, 0, stream>>>(g);
     }
     int st = check_launch("det/csf transform");

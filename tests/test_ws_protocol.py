@@ -101,7 +101,7 @@ def _run(rows, nwm, nmov, seed, tails=()):
 
 @pytest.mark.parametrize("nwm,nmov", [(17, 3), (16, 4), (15, 5), (12, 4), (3, 2)])
 def test_ws_barrier_protocol(nwm, nmov):
-    for rows in ([1], [2], [3], [1, 4, 2, 7, 3], [5, 1, 1, 6], [10, 9, 8]):
+    for rows in ([1], [2], [3], [1, 4, 2, 7, 3], [5, 1, 1, 6], [10, 9, 8], [0, 3, 0, 0, 2], [0]):
         for seed in range(25):
             _run(rows, nwm, nmov, seed)
 
