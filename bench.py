@@ -49,7 +49,8 @@ WORKLOADS = {"cas16": (16, (8, 8), 32), "cas14": (14, (7, 7), 28), "cas12": (12,
 # one ncu capture of the dram byte counters on the full-size launch; None
 # for what was not captured
 TRAFFIC = {("cas16", "k_sigma_rr"): 26934597120 + 13410886400,
-           ("cas16", "k_sigma_ws"): 33107436032 + 16856211456}
+           ("cas16", "k_sigma_ws"): 33107436032 + 16856211456,
+           ("cas16", "k_sigma_wsr"): 39177203456 + 19706565376}
 
 
 def seeded_integrals(norb, rank, seed=0):

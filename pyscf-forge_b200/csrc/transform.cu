@@ -218,6 +218,76 @@ static bool small_block(const csffci_block_t& B) {
          B.ndet <= 256;
 }
 
+// det -> CSF blocks with few (vector, configuration) rows and a long K (at
+// CAS(16,16) npair 0: 1 configuration x 12870 determinants x 1430 CSFs, and
+// npair 1: 240 x 3432 x 429): the 64 x 64 GEMM tiles leave most SMs idle
+// and walk K alone.  Here a CTA takes 16 rows x 32 CSF columns and its 8
+// warps split K: the rows' gathered determinant values are staged in shared
+// memory a chunk of K at a time (coalesced mask reads, independent
+// gathers), each lane keeps the 16 sums of its column, and the 8 warp
+// partials are added in a fixed order at the end.
+constexpr int TK_M = 16, TK_N = 32, TK_KC = 512, TK_W = 8;
+
+constexpr size_t TK_SMEM = (size_t)TK_M * TK_KC * sizeof(double);  // 64 KB (dynamic)
+static_assert((size_t)TK_W * TK_M * (TK_N + 1) * sizeof(double) <= TK_SMEM, "the partials reuse the chunk buffer");
+
+__global__ void __launch_bounds__(TK_W * 32) k_block_tallk(BlockGemmArgs g) {
+  extern __shared__ double tk_smem[];
+  double (*Xs)[TK_KC] = reinterpret_cast<double (*)[TK_KC]>(tk_smem);              // gathered chunk
+  double (*Ps)[TK_M][TK_N + 1] = reinterpret_cast<double (*)[TK_M][TK_N + 1]>(tk_smem);  // warp partials
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t M = (int64_t)g.nvec * g.nconf;
+  const int N = g.ncsf, K = g.ndet;
+  const int ntn = (N + TK_N - 1) / TK_N;
+  const int64_t ntiles = ((M + TK_M - 1) / TK_M) * ntn;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t m0 = (tile / ntn) * TK_M;
+    const int n0 = (int)(tile % ntn) * TK_N;
+    const int n = n0 + lane;
+    double acc[TK_M];
+#pragma unroll
+    for (int i = 0; i < TK_M; ++i) acc[i] = 0.0;
+    for (int k0 = 0; k0 < K; k0 += TK_KC) {
+      const int kc = min(TK_KC, K - k0);
+      __syncthreads();  // the previous chunk is consumed
+      for (int e = tid; e < TK_M * TK_KC; e += TK_W * 32) {
+        const int r = e / TK_KC, kk = e - r * TK_KC;
+        const int64_t m = m0 + r;
+        double v = 0.0;
+        if (m < M && kk < kc) {
+          const int64_t vec = m / g.nconf, conf = m - vec * g.nconf;
+          const int64_t cf = g.conf_sel ? g.conf_sel[conf] : conf;
+          v = g.x[vec * g.ldx + g.mask[g.csd_off + cf * g.ndet + k0 + kk]];
+        }
+        Xs[r][kk] = v;
+      }
+      __syncthreads();
+      const int kw = (kc + TK_W - 1) / TK_W;  // k per warp in this chunk
+      const int kb = warp * kw, ke = min(kc, kb + kw);
+      if (n < N)
+        for (int kk = kb; kk < ke; ++kk) {
+          const double u = g.umat[(int64_t)(k0 + kk) * N + n];
+#pragma unroll
+          for (int i = 0; i < TK_M; ++i) acc[i] = fma(Xs[i][kk], u, acc[i]);
+        }
+    }
+    __syncthreads();  // every warp is done with the last chunk (Ps overlays Xs)
+#pragma unroll
+    for (int i = 0; i < TK_M; ++i) Ps[warp][i][lane] = acc[i];
+    __syncthreads();
+    for (int e = tid; e < TK_M * TK_N; e += TK_W * 32) {
+      const int i = e / TK_N, j = e - i * TK_N;
+      const int64_t m = m0 + i;
+      if (m >= M || n0 + j >= N) continue;
+      double v = 0.0;
+#pragma unroll
+      for (int w = 0; w < TK_W; ++w) v += Ps[w][i][j];
+      const int64_t vec = m / g.nconf, conf = m - vec * g.nconf;
+      g.y[vec * g.ldy + g.csf_off + conf * N + n0 + j] = g.sign * v;
+    }
+  }
+}
+
 __global__ void k_zero_rows(double* y, int64_t ldy, int nvec, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)nvec * n;
        i += (int64_t)gridDim.x * blockDim.x) {
@@ -257,6 +327,18 @@ static int run_blocks(int nvec, const double* x, int64_t ldx, double* y, int64_t
     int64_t M = (int64_t)nvec * B.nconf;
     int N = (MODE == MODE_DET2CSF) ? B.ncsf : B.ndet;
     int64_t tiles = ((M + TBM - 1) / TBM) * ((N + TBN - 1) / TBN);
+    if (MODE == MODE_DET2CSF && tiles < 2 * 148 && B.ndet >= 4 * TK_KC) {
+      // few GEMM tiles over a long K: the K-split kernel
+      const int64_t tk = ((M + TK_M - 1) / TK_M) * ((N + TK_N - 1) / TK_N);
+      CSF_CUDA(cudaFuncSetAttribute(k_block_tallk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TK_SMEM));
+      {
+        ProfScope ps_(block_kernel_name(false, B.npair), stream);
+        k_block_tallk<<<grid_for(tk, 1, 148 * 3), TK_W * 32, TK_SMEM, stream>>>(g);
+      }
+      const int st = check_launch("det->CSF transform (long K)");
+      if (st) return st;
+      continue;
+    }
     {
       ProfScope ps_(block_kernel_name(false, B.npair), stream);
       k_block_gemm<MODE><<<grid_for(tiles, 1, 148 * 8), 256, 0, stream>>>(g);
