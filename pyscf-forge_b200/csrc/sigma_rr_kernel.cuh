@@ -33,7 +33,8 @@ struct RRArgs {
   unsigned off_extra;  // register-split kernel: tail partial sums
   unsigned off_mbar;   // warp-specialised kernels: one mbarrier per stage
   int bulk;            // warp-specialised kernels: alpha rows by bulk copy
-  int parts;           // warp-specialised kernels: parts per row unit (tile ranges)
+  int parts;           // warp-specialised kernels: parts of each row unit from split_from on
+  long long split_from;  // warp-specialised kernels: first row unit cut into parts
 };
 
 // Alpha link of the current row Ja as the tile loops use it: the offset

@@ -193,6 +193,7 @@ static int launch_ws(RRArgs& g, size_t smem, cudaStream_t stream) {
     return CSFFCI_ERR_INVALID;
   }
   long long grid = (long long)nsm * per_sm;
+  ws_split_last_round(g, grid);
   if (grid > g.total_units) grid = g.total_units;
   if (grid < 1) return CSFFCI_OK;
   ProfScope ps("k_sigma_ws", stream);
@@ -242,11 +243,9 @@ int sigma_ws_launch(int norb, const csffci_sigma_job_t& job0, long long total_un
   g.jobs = nullptr;
   g.job0 = job0;
   g.njobs = 1;
-  // spin-symmetric row units (pairs of rows of equal total length) are cut
-  // in two tile ranges: 2 x (Na+1)/2 units balance the 148 SMs to within a
-  // fraction of a unit
-  g.parts = job0.sym ? 2 : 1;
-  g.total_units = total_units * g.parts;
+  g.parts = 1;
+  g.split_from = total_units;
+  g.total_units = total_units;
   const size_t smem = ws_layout(g, npair, 8, max_nb, max_nla, max_nlb, 0, nullptr);
   if (smem == 0) {
     set_error("sigma: warp-specialised tiles exceed shared memory (norb %d)", norb);

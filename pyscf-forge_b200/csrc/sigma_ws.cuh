@@ -98,17 +98,24 @@ struct WSShared {
 // same arguments, and it synchronises the CTA on barrier 9): the alpha links
 // of row Ja, the rows without one, the sign masks of this row (in half par
 // of pneg) and the copy of c row Ja.  Returns false (for every thread) when
-// the spin-symmetric unit has no second row.  A unit (index iu) is part
-// iu % g.parts of row unit iu / g.parts: the tiles [c0, c0 + nchunk) of the
-// row, so that units are small enough to balance the SMs.
+// the spin-symmetric unit has no second row.  Units below g.split_from are
+// whole row units; from there on (the last, partial round of the grid) a
+// unit is one of g.parts tile ranges [c0, c0 + nchunk) of a row unit, so
+// that the last round spreads over every SM.
 template <int NTH, int NB>
 __device__ __forceinline__ bool ws_row_setup(const RRArgs& g, const WSShared& S, long long iu, int w, int par,
                                              int tid, int warp, int lane) {
   const csffci_sigma_job_t& sjob = g.job0;
   const long long Nb = sjob.Nb;
   const int nla = sjob.nla, npair = g.npair, ds = g.ds;
-  const long long lu = iu / g.parts;
-  const int part = (int)(iu - lu * g.parts);
+  long long lu = iu;
+  int part = 0, parts = 1;
+  if (iu >= g.split_from) {  // two tile ranges per row unit
+    const long long r = iu - g.split_from;
+    lu = g.split_from + (r >> 1);
+    part = (int)(r & 1);
+    parts = 2;
+  }
   long long ja = lu;
   if (sjob.sym && w == 1) {
     ja = sjob.Na - 1 - lu;
@@ -120,8 +127,8 @@ __device__ __forceinline__ bool ws_row_setup(const RRArgs& g, const WSShared& S,
     S.srow->ja = ja;
     S.srow->jend = sjob.sym ? ja + 1 : Nb;
     const int nt = (int)((S.srow->jend + NB - 1) / NB);
-    S.srow->c0 = (int)((long long)part * nt / g.parts);
-    S.srow->nchunk = (int)((long long)(part + 1) * nt / g.parts) - S.srow->c0;
+    S.srow->c0 = parts == 2 && part ? nt / 2 : 0;
+    S.srow->nchunk = parts == 2 && !part ? nt / 2 : nt - S.srow->c0;
     S.srow->pc = par * npair;
   }
   for (int r = tid; r < npair; r += NTH) {
@@ -325,6 +332,20 @@ __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S
 // offset returned in *extra_off).  Returns 0 when it does not fit.
 size_t ws_layout(RRArgs& g, int npair, int rows_multiple, long long max_nb, int max_nla, int max_nlb,
                  size_t extra_bytes, unsigned* extra_off);
+
+// The grid strides over the row units, so with nru units and a grid of G
+// CTAs the last round has nru % G units and leaves the other SMs idle for
+// a whole unit.  Those units are cut in two tile ranges each: the last
+// round then spreads over twice as many CTAs.  The earlier units stay whole
+// (every unit reloads its row of c, so cutting them all would double that).
+inline void ws_split_last_round(RRArgs& g, long long grid) {
+  const long long nru = g.total_units;
+  const long long tail = grid > 0 ? nru % grid : 0;
+  if (nru <= grid || tail == 0) return;
+  g.split_from = nru - tail;
+  g.parts = 2;  // ws_row_setup cuts these units in two
+  g.total_units = g.split_from + tail * 2;
+}
 
 // whether the alpha rows of one problem can go through the bulk-copy
 // engine: 16-byte aligned rows of c (ci 16-byte aligned, Nb even)

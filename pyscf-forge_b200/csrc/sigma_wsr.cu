@@ -289,8 +289,9 @@ int sigma_wsr_launch(int norb, const csffci_sigma_job_t& job0, long long total_u
   g.jobs = nullptr;
   g.job0 = job0;
   g.njobs = 1;
-  g.parts = job0.sym ? 2 : 1;  // as in sigma_ws_launch
-  g.total_units = total_units * g.parts;
+  g.parts = 1;
+  g.split_from = total_units;
+  g.total_units = total_units;
   unsigned extra = 0;
   const size_t smem = ws_layout(g, npair, 8, max_nb, max_nla, max_nlb, 4 * 64 * sizeof(double), &extra);
   if (smem == 0) {
@@ -320,6 +321,7 @@ int sigma_wsr_launch(int norb, const csffci_sigma_job_t& job0, long long total_u
     return CSFFCI_ERR_INVALID;
   }
   long long grid = nsm;
+  ws_split_last_round(g, grid);
   if (grid > g.total_units) grid = g.total_units;
   if (grid < 1) return CSFFCI_OK;
   ProfScope ps(g.bulk ? "k_sigma_wsr_bulk" : "k_sigma_wsr", stream);
