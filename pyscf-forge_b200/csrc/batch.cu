@@ -25,7 +25,62 @@ __device__ __forceinline__ int find_job(const int64_t* begin, int njobs, int64_t
   return j;
 }
 
-// One tile = 32 (vec, conf) rows x 32 output columns of one job.
+// Blocks with few CSFs (ncsf <= BR_MAX_NCSF) and few determinants per
+// configuration are most of the determinants below 13 orbitals (norb 12,
+// (6,6): 92 % of them in blocks of 6..70 determinants and 2..14 CSFs), and
+// a 32 x 32 output tile would leave most of its columns empty there.  Such
+// a job is cut into units of 256 (vector, configuration) rows instead, one
+// row per thread: the row's determinants are gathered through its mask
+// row and contracted with umat (read as warp-uniform loads: every thread
+// of a unit is in the same job) into NC register sums.  The sums run over
+// k in increasing order with fma, as the tile path's do, so both paths give
+// the same bits.
+constexpr int BR_ROWS = 256, BR_MAX_NCSF = 16, BR_MAX_NDET = 256;
+
+__host__ __device__ inline bool row_job(const csffci_transform_job_t& J) {
+  return J.ncsf <= BR_MAX_NCSF && J.ndet <= BR_MAX_NDET;
+}
+
+template <int NC>
+__device__ __forceinline__ void transform_row(const csffci_transform_job_t& J, int64_t vec, int64_t conf,
+                                              int reverse) {
+  const int nd = J.ndet, nc = J.ncsf;
+  const uint32_t* mk = J.mask + J.csd_offset + conf * nd;
+  if (!reverse) {
+    double acc[NC];
+#pragma unroll
+    for (int k = 0; k < NC; ++k) acc[k] = 0.0;
+    const double* xv = J.x + vec * J.ldx;
+    for (int d = 0; d < nd; ++d) {
+      const double v = xv[mk[d]];
+      const double* u = J.umat + (int64_t)d * nc;
+#pragma unroll
+      for (int k = 0; k < NC; ++k)
+        if (k < nc) acc[k] = fma(v, u[k], acc[k]);
+    }
+    double* yo = J.y + vec * J.ldy + J.csf_offset + conf * nc;
+#pragma unroll
+    for (int k = 0; k < NC; ++k)
+      if (k < nc) yo[k] = J.sign * acc[k];
+  } else {
+    double cin[NC];
+    const double* xi = J.x + vec * J.ldx + J.csf_offset + conf * nc;
+#pragma unroll
+    for (int k = 0; k < NC; ++k) cin[k] = k < nc ? xi[k] : 0.0;
+    double* yv = J.y + vec * J.ldy;
+    for (int d = 0; d < nd; ++d) {
+      const double* u = J.umat + (int64_t)d * nc;
+      double acc = 0.0;
+#pragma unroll
+      for (int k = 0; k < NC; ++k)
+        if (k < nc) acc = fma(cin[k], u[k], acc);
+      yv[mk[d]] = J.sign * acc;
+    }
+  }
+}
+
+// One tile = 32 (vec, conf) rows x 32 output columns of one job, or, for a
+// row job, 256 rows.
 __global__ void __launch_bounds__(256) k_transform_batch(const csffci_transform_job_t* jobs, int njobs,
                                                          int64_t total_tiles, int reverse) {
   __shared__ double As[BT_K][BT_M + 1];
@@ -37,10 +92,22 @@ __global__ void __launch_bounds__(256) k_transform_batch(const csffci_transform_
     const csffci_transform_job_t& J = jobs[j];
     const int nv = J.live ? min(J.nvec, *J.live) : J.nvec;
     const int64_t M = (int64_t)nv * J.nconf;
+    const int64_t lt = tile - J.tile_begin;
+    if (row_job(J)) {
+      const int64_t m = lt * BR_ROWS + tid;
+      if (m < M) {
+        const csffci_transform_job_t Jr = J;  // in registers: the stores below cannot alias it
+        const int64_t vec = m / Jr.nconf, conf = m - vec * Jr.nconf;
+        if (Jr.ncsf <= 2) transform_row<2>(Jr, vec, conf, reverse);
+        else if (Jr.ncsf <= 4) transform_row<4>(Jr, vec, conf, reverse);
+        else if (Jr.ncsf <= 8) transform_row<8>(Jr, vec, conf, reverse);
+        else transform_row<BR_MAX_NCSF>(Jr, vec, conf, reverse);
+      }
+      continue;
+    }
     const int N = reverse ? J.ndet : J.ncsf;
     const int K = reverse ? J.ncsf : J.ndet;
     const int ntn = (N + BT_N - 1) / BT_N;
-    const int64_t lt = tile - J.tile_begin;
     const int64_t m0 = (lt / ntn) * BT_M;
     const int n0 = (int)(lt % ntn) * BT_N;
     if (m0 >= M) continue;  // rows of vectors that are not live (uniform per block)
@@ -196,7 +263,7 @@ int transform_batch_prepare(int reverse, int njobs, csffci_transform_job_t* jobs
     J.tile_begin = tiles;
     const int64_t M = (int64_t)J.nvec * J.nconf;
     const int N = reverse ? J.ndet : J.ncsf;
-    tiles += ((M + BT_M - 1) / BT_M) * ((N + BT_N - 1) / BT_N);
+    tiles += row_job(J) ? (M + BR_ROWS - 1) / BR_ROWS : ((M + BT_M - 1) / BT_M) * ((N + BT_N - 1) / BT_N);
   }
   *total_tiles = tiles;
   return CSFFCI_OK;

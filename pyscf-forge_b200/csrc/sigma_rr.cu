@@ -42,17 +42,23 @@ static bool rr_aligned8(const void* p) { return ((uintptr_t)p & 7u) == 0; }
 // Tile shapes (rows per warp, n-tiles of 8 columns): 16-row warps halve
 // the B-fragment traffic but need 2*KS + 4*NT doubles of registers per lane;
 // with 9 warps (norb 15,16) an SMSP holds 3 warps, i.e. at most 168
-// registers, so those sizes have no (16, 4) instance.  The defaults are the
-// fastest shapes measured on B200 for one singlet/doublet problem: (16, 2)
-// up to norb 10 and at 13, (8, 2) for 11-12, (8, 4) from 14 (the two-n-tile
-// shapes run 2-3 CTAs per SM at small norb); CSFFCI_SIGMA_VARIANT overrides them
-// and the batched solver's autotuner picks per orbital count.
+// registers, so those sizes have no (16, 4) instance.  Where the
+// warp-specialised kernel is not the default (rr_default_variant), the
+// fastest shapes measured on B200 for one singlet/doublet problem are
+// (16, 2) up to norb 10 and at 13, (8, 2) for 11-12, (8, 4) from 14 (the
+// two-n-tile shapes run 2-3 CTAs per SM at small norb); CSFFCI_SIGMA_VARIANT
+// overrides the choice and the batched solver's autotuner picks per orbital
+// count.
 static const int kVariantShape[RR_NVARIANT][2] = {{16, 4}, {8, 4}, {16, 2}, {8, 2}};
 
 bool rr_variant_valid(int norb, int v) { return v >= 0 && v < RR_NVARIANT && !(v == 0 && norb >= 15); }
 
-// one problem: the warp-specialised kernel from 14 orbitals (CSFFCI_SIGMA_VARIANT
-// may name any variant); -1 leaves the choice to rr_default_variant
+bool batch_variant_valid(int norb, int v) {
+  return rr_variant_valid(norb, v) || (v == RR_VARIANT_WS && sigma_ws_supported(norb));
+}
+
+// one problem: the register-split kernel at 16 orbitals, else the job-table
+// default (CSFFCI_SIGMA_VARIANT may name any variant)
 int sigma_rr_single_variant(int norb) {
   const char* env = getenv("CSFFCI_SIGMA_VARIANT");
   if (env) {
@@ -61,20 +67,29 @@ int sigma_rr_single_variant(int norb) {
     if ((v == RR_VARIANT_WSR || v == RR_VARIANT_WSR_BULK) && sigma_wsr_supported(norb)) return v;
     if (rr_variant_valid(norb, v)) return v;
   }
-  // measured on B200 (singlet, one problem): 14 orbitals 7.61 -> 6.31 ms,
-  // 15: 31.1 -> 25.8 ms, 16: 148.8 -> 129.5 ms (k_sigma_ws) and 119 ms
-  // (k_sigma_wsr, registers re-split between the roles); at 13 the
-  // warp-specialised kernel is no faster
+  // measured on B200 (one problem), best tile shape -> k_sigma_ws: 10
+  // orbitals (5,5) singlet 0.044 -> 0.042 ms, 11 (6,5) 0.191 -> 0.167 ms,
+  // 12 (6,6) singlet 0.444 -> 0.349 ms, 12 (7,6) 0.572 -> 0.507 ms, 14
+  // singlet 7.61 -> 6.31 ms, 15: 31.1 -> 25.8 ms, 16: 148.8 -> 129.5 ms and
+  // 116 ms (k_sigma_wsr, registers re-split between the roles); at 13 the
+  // warp-specialised kernel is no faster, at 9 and below the tile shapes
+  // are faster
   if (sigma_wsr_supported(norb)) return RR_VARIANT_WSR;
-  return norb >= 14 && sigma_ws_supported(norb) ? RR_VARIANT_WS : -1;
+  return rr_default_variant(norb);
 }
 
+// job tables (and one problem below 16 orbitals): the warp-specialised
+// kernel at 10..12 and 14..16 orbitals (the C3 batch of 128 problems: norb
+// 12 jobs 24.6 -> 23.2 ms per launch, norb 11 4.40 -> 3.99 ms, norb 10
+// 0.89 -> 0.85 ms against the best tile shape); the batched solver's
+// autotuner times every variant on its own job tables
 int rr_default_variant(int norb) {
   const char* env = getenv("CSFFCI_SIGMA_VARIANT");
   if (env) {
     const int v = atoi(env);
-    if (rr_variant_valid(norb, v)) return v;
+    if (batch_variant_valid(norb, v)) return v;
   }
+  if (norb >= 10 && norb != 13 && sigma_ws_supported(norb)) return RR_VARIANT_WS;
   return norb <= 10 || norb == 13 ? 2 : norb <= 12 ? 3 : 1;
 }
 
@@ -111,13 +126,8 @@ int sigma_rr_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev,
   const int ks = (npair + 3) / 4;
   if (variant < 0 && !jobs_dev) variant = sigma_rr_single_variant(norb);
   if (variant < 0) variant = rr_default_variant(norb);
-  if (variant == RR_VARIANT_WS) {
-    if (jobs_dev) {
-      set_error("sigma: the warp-specialised variant takes one problem, not a job table");
-      return CSFFCI_ERR_INVALID;
-    }
-    return sigma_ws_launch(norb, job0, total_units, max_nb, max_nla, max_nlb, stream);
-  }
+  if (variant == RR_VARIANT_WS)
+    return sigma_ws_launch(norb, njobs, jobs_dev, job0, total_units, max_nb, max_nla, max_nlb, stream);
   if (variant == RR_VARIANT_WSR || variant == RR_VARIANT_WSR_BULK) {
     if (jobs_dev) {
       set_error("sigma: the register-split variant takes one problem, not a job table");
@@ -320,8 +330,8 @@ int sigma_batch_tune(SigmaBatchInfo& info, const csffci_sigma_job_t* jobs_host, 
   CSF_CUDA(cudaEventCreate(&b));
   int best = rr_default_variant(info.norb);
   float best_ms = 1e30f;
-  for (int v = 0; v < RR_NVARIANT; ++v) {
-    if (!rr_variant_valid(info.norb, v)) continue;
+  for (int v = 0; v <= RR_VARIANT_WS; ++v) {
+    if (!batch_variant_valid(info.norb, v)) continue;
     SigmaBatchInfo t = info;
     t.variant = v;
     if (sigma_batch_launch(t, dj, stream) != CSFFCI_OK) continue;  // e.g. shared memory too small

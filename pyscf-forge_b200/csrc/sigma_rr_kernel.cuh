@@ -419,11 +419,12 @@ static int launch_rr(RRArgs& g, size_t smem, cudaStream_t stream) {
 
 // tile-shape variants: (rows per warp, n-tiles of 8 columns)
 constexpr int RR_NVARIANT = 4;
-// the warp-specialised kernel (sigma_ws.cu), one problem at 13..16 orbitals
+// the warp-specialised kernel (sigma_ws.cu), 8..16 orbitals, one problem
+// or a job table
 constexpr int RR_VARIANT_WS = 4;
 bool sigma_ws_supported(int norb);
-int sigma_ws_launch(int norb, const csffci_sigma_job_t& job0, long long total_units, long long max_nb,
-                    int max_nla, int max_nlb, cudaStream_t stream);
+int sigma_ws_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev, const csffci_sigma_job_t& job0,
+                    long long total_units, long long max_nb, int max_nla, int max_nlb, cudaStream_t stream);
 // the warp-specialised kernel with registers re-split between the roles
 // (sigma_wsr.cu), one problem at 16 orbitals
 constexpr int RR_VARIANT_WSR = 5;
@@ -433,6 +434,8 @@ bool sigma_wsr_supported(int norb);
 int sigma_wsr_launch(int norb, const csffci_sigma_job_t& job0, long long total_units, long long max_nb,
                      int max_nla, int max_nlb, cudaStream_t stream, bool bulk);
 bool rr_variant_valid(int norb, int v);
+// the variants a job table may run: the tile shapes and the warp-specialised kernel
+bool batch_variant_valid(int norb, int v);
 int rr_default_variant(int norb);
 int sigma_rr_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev, const csffci_sigma_job_t& job0,
                     long long total_units, long long max_nb, int max_nla, int max_nlb, cudaStream_t stream,

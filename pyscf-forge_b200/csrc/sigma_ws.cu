@@ -54,8 +54,8 @@ struct WSLayout {
 
 constexpr int WS_RU = 4;      // links a mover thread handles together (loads in flight)
 
-template <int KS, int MT>
-__global__ void __launch_bounds__(WSLayout<MT>::NTOT * 32, 1) k_sigma_ws(RRArgs g) {
+template <int KS, int MT, bool BATCH, int MINB>
+__global__ void __launch_bounds__(WSLayout<MT>::NTOT * 32, MINB) k_sigma_ws(RRArgs g) {
   using L = WSLayout<MT>;
   constexpr int NB = WS_NB;
   constexpr int NTH = L::NTOT * 32;
@@ -73,9 +73,13 @@ __global__ void __launch_bounds__(WSLayout<MT>::NTOT * 32, 1) k_sigma_ws(RRArgs 
   S.srow = &srow;
   S.apoff = (long long*)(smraw + g.off_ap);
   S.mbar = (unsigned long long*)(smraw + g.off_mbar);
-  const csffci_sigma_job_t& sjob = g.job0;
+  __shared__ csffci_sigma_job_t sjob_s;
+  __shared__ int jst[2];
+  S.job = &sjob_s;
+  S.jst = jst;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (BATCH && tid == 0) jst[0] = -1;  // ordered before its first use by barrier 9
   if (g.bulk && tid == 0) {
     for (int s = 0; s < WS_STAGES; ++s) ws_mbar_init(&S.mbar[s], 1);
     ws_mbar_init_fence();  // the row setup's barriers order it before every use
@@ -93,20 +97,33 @@ __global__ void __launch_bounds__(WSLayout<MT>::NTOT * 32, 1) k_sigma_ws(RRArgs 
     const int mt = part ? 4 * L::q + (warp - 4 * L::q) / 2 : warp;
     const int t0 = part ? (warp - 4 * L::q) % 2 : 0;
     double a0f[KS];
-    {
+    // h2e rows 8 mt + g of the job, columns 4k + t (without signs)
+    auto load_a = [&](const double* h2e) {
       const int r0 = mt * 8 + gq;
 #pragma unroll
       for (int k = 0; k < KS; ++k) {
         const int c = 4 * k + tq;
-        a0f[k] = (r0 < npair && c < npair) ? sjob.h2e[(long long)r0 * npair + c] : 0.0;
+        a0f[k] = (r0 < npair && c < npair) ? h2e[(long long)r0 * npair + c] : 0.0;
       }
-    }
-    bool fresh = true;
+    };
+    if (!BATCH) load_a(g.job0.h2e);
+    int cur = -1;       // job table index whose h2e the registers hold
+    bool fresh = true;  // a0f holds h2e without signs
     int par = 0;
     for (long long u = blockIdx.x; u < g.total_units; u += gridDim.x) {
-      const long long lu = u - sjob.unit_begin;
+      const WSUnit un = ws_unit(g, u);
+      if (BATCH) {
+        if (!ws_batch_job<NTH>(g, S, un.ru, tid)) continue;
+        if (jst[0] != cur) {
+          cur = jst[0];
+          load_a(sjob_s.h2e);
+          fresh = true;
+        }
+      }
+      const csffci_sigma_job_t& sjob = BATCH ? sjob_s : g.job0;
+      const long long lu = un.ru - sjob.unit_begin;
       for (int w = 0; w < (sjob.sym ? 2 : 1); ++w) {
-        if (!ws_row_setup<NTH, NB>(g, S, lu, w, par, tid, warp, lane)) break;
+        if (!ws_row_setup<NTH, NB>(g, S, sjob, lu, un.part, un.parts, w, par, tid, warp, lane)) break;
         {
           // sign columns of A where this row's alpha sign differs from the
           // one the registers carry
@@ -173,16 +190,22 @@ __global__ void __launch_bounds__(WSLayout<MT>::NTOT * 32, 1) k_sigma_ws(RRArgs 
       }
     }
   } else {
-    ws_mover_role<NTH, NMOV, WS_RU>(g, S, tid, warp, lane, tid - NWM * 32, warp - NWM);
+    ws_mover_role<NTH, NMOV, WS_RU, BATCH>(g, S, tid, warp, lane, tid - NWM * 32, warp - NWM);
   }
 }
 
-bool sigma_ws_supported(int norb) { return norb >= 13 && norb <= 16; }
+bool sigma_ws_supported(int norb) { return norb >= 8 && norb <= 16; }
 
-template <int KS, int MT>
+// CTAs per SM the registers are sized for: below 13 orbitals the A
+// fragments are small enough for two CTAs per SM, so that one CTA's row
+// setup (barrier 9) overlaps the other's tiles
+constexpr int ws_min_blocks(int norb) { return norb <= 12 ? 2 : 1; }
+
+template <int KS, int MT, int NORB>
 static int launch_ws(RRArgs& g, size_t smem, cudaStream_t stream) {
   constexpr int NTH = WSLayout<MT>::NTOT * 32;
-  auto kern = k_sigma_ws<KS, MT>;
+  constexpr int MINB = ws_min_blocks(NORB);
+  auto kern = g.jobs ? k_sigma_ws<KS, MT, true, MINB> : k_sigma_ws<KS, MT, false, MINB>;
   CSF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, nsm = 148, per_sm = 0;
   CSF_CUDA(cudaGetDevice(&dev));
@@ -196,7 +219,10 @@ static int launch_ws(RRArgs& g, size_t smem, cudaStream_t stream) {
   ws_split_last_round(g, grid);
   if (grid > g.total_units) grid = g.total_units;
   if (grid < 1) return CSFFCI_OK;
-  ProfScope ps("k_sigma_ws", stream);
+  static const char* names[17] = {"", "", "", "", "", "", "", "", "k_sigma_ws_n8", "k_sigma_ws_n9",
+                                  "k_sigma_ws_n10", "k_sigma_ws_n11", "k_sigma_ws_n12", "k_sigma_ws_n13",
+                                  "k_sigma_ws_n14", "k_sigma_ws_n15", "k_sigma_ws_n16"};
+  ProfScope ps(g.jobs ? names[NORB] : "k_sigma_ws", stream);
   kern<<<(int)grid, NTH, smem, stream>>>(g);
   return check_launch("sigma (warp-specialised)");
 }
@@ -231,18 +257,18 @@ size_t ws_layout(RRArgs& g, int npair, int rows_multiple, long long max_nb, int 
   return off > 227 * 1024 - 256 ? 0 : off;
 }
 
-int sigma_ws_launch(int norb, const csffci_sigma_job_t& job0, long long total_units, long long max_nb,
-                    int max_nla, int max_nlb, cudaStream_t stream) {
+int sigma_ws_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev, const csffci_sigma_job_t& job0,
+                    long long total_units, long long max_nb, int max_nla, int max_nlb, cudaStream_t stream) {
   if (!sigma_ws_supported(norb)) {
-    set_error("sigma: the warp-specialised variant covers norb 13..16, not %d", norb);
+    set_error("sigma: the warp-specialised variant covers norb 8..16, not %d", norb);
     return CSFFCI_ERR_INVALID;
   }
   const int npair = norb * (norb + 1) / 2;
   RRArgs g;
   memset(&g, 0, sizeof(g));
-  g.jobs = nullptr;
+  g.jobs = jobs_dev;
   g.job0 = job0;
-  g.njobs = 1;
+  g.njobs = jobs_dev ? njobs : 1;
   g.parts = 1;
   g.split_from = total_units;
   g.total_units = total_units;
@@ -251,11 +277,16 @@ int sigma_ws_launch(int norb, const csffci_sigma_job_t& job0, long long total_un
     set_error("sigma: warp-specialised tiles exceed shared memory (norb %d)", norb);
     return CSFFCI_ERR_INVALID;
   }
-  switch (norb) {
-    case 13: return launch_ws<23, 12>(g, smem, stream);
-    case 14: return launch_ws<27, 14>(g, smem, stream);
-    case 15: return launch_ws<30, 15>(g, smem, stream);
-    default: return launch_ws<34, 17>(g, smem, stream);
+  switch (norb) {  // KS = ceil(npair / 4), MT = ceil(npair / 8)
+    case 8: return launch_ws<9, 5, 8>(g, smem, stream);
+    case 9: return launch_ws<12, 6, 9>(g, smem, stream);
+    case 10: return launch_ws<14, 7, 10>(g, smem, stream);
+    case 11: return launch_ws<17, 9, 11>(g, smem, stream);
+    case 12: return launch_ws<20, 10, 12>(g, smem, stream);
+    case 13: return launch_ws<23, 12, 13>(g, smem, stream);
+    case 14: return launch_ws<27, 14, 14>(g, smem, stream);
+    case 15: return launch_ws<30, 15, 15>(g, smem, stream);
+    default: return launch_ws<34, 17, 16>(g, smem, stream);
   }
 }
 

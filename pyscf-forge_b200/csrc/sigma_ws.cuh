@@ -92,30 +92,67 @@ struct WSShared {
   RRRow* srow;
   long long* apoff;  // per pair row: Ka*Nb of its alpha link in row Ja, -1 without one
   unsigned long long* mbar;  // one mbarrier per stage (bulk alpha-row copies)
+  csffci_sigma_job_t* job;   // job-table kernels: the current unit's job ...
+  int* jst;                  // ... its index in the table and whether it is live
 };
+
+// One step of the grid-stride loop: row unit ru and, from g.split_from on
+// (the last, partial round of the grid), which of two tile ranges of it.
+struct WSUnit {
+  long long ru;
+  int part, parts;
+};
+
+__device__ __forceinline__ WSUnit ws_unit(const RRArgs& g, long long u) {
+  WSUnit r;
+  r.ru = u;
+  r.part = 0;
+  r.parts = 1;
+  if (u >= g.split_from) {  // two tile ranges per row unit
+    const long long k = u - g.split_from;
+    r.ru = g.split_from + (k >> 1);
+    r.part = (int)(k & 1);
+    r.parts = 2;
+  }
+  return r;
+}
+
+// Job-table kernels: thread 0 finds the job that owns row unit ru (units
+// only grow along a CTA's loop, so the search goes forward from the last
+// job) and copies it to shared memory; both roles call this with the same
+// ru and return the same answer: whether the job is live (a gated job, whose
+// problem has no new vector this iteration, is skipped as a whole).
+template <int NTH>
+__device__ __forceinline__ bool ws_batch_job(const RRArgs& g, const WSShared& S, long long ru, int tid) {
+  ws_bar_sync(9, NTH);  // every thread is done with the previous unit's job record
+  if (tid == 0) {
+    int j = S.jst[0] < 0 ? 0 : S.jst[0];
+    while (j + 1 < g.njobs && g.jobs[j + 1].unit_begin <= ru) ++j;
+    if (j != S.jst[0]) {
+      *S.job = g.jobs[j];
+      S.jst[0] = j;
+    }
+    const csffci_sigma_job_t& J = *S.job;
+    S.jst[1] = J.live == nullptr || J.live_index < *J.live;
+  }
+  ws_bar_sync(9, NTH);
+  return S.jst[1] != 0;
+}
 
 // Row setup shared by both roles (every thread of the CTA calls it with the
 // same arguments, and it synchronises the CTA on barrier 9): the alpha links
 // of row Ja, the rows without one, the sign masks of this row (in half par
 // of pneg) and the copy of c row Ja.  Returns false (for every thread) when
-// the spin-symmetric unit has no second row.  Units below g.split_from are
-// whole row units; from there on (the last, partial round of the grid) a
-// unit is one of g.parts tile ranges [c0, c0 + nchunk) of a row unit, so
-// that the last round spreads over every SM.
+// the spin-symmetric unit has no second row.  lu is the job's own row unit;
+// a unit of the last, partial round of the grid (parts == 2) is one of two
+// tile ranges [c0, c0 + nchunk) of it, so that the last round spreads over
+// every SM.
 template <int NTH, int NB>
-__device__ __forceinline__ bool ws_row_setup(const RRArgs& g, const WSShared& S, long long iu, int w, int par,
-                                             int tid, int warp, int lane) {
-  const csffci_sigma_job_t& sjob = g.job0;
+__device__ __forceinline__ bool ws_row_setup(const RRArgs& g, const WSShared& S, const csffci_sigma_job_t& sjob,
+                                             long long lu, int part, int parts, int w, int par, int tid,
+                                             int warp, int lane) {
   const long long Nb = sjob.Nb;
   const int nla = sjob.nla, npair = g.npair, ds = g.ds;
-  long long lu = iu;
-  int part = 0, parts = 1;
-  if (iu >= g.split_from) {  // two tile ranges per row unit
-    const long long r = iu - g.split_from;
-    lu = g.split_from + (r >> 1);
-    part = (int)(r & 1);
-    parts = 2;
-  }
   long long ja = lu;
   if (sjob.sym && w == 1) {
     ja = sjob.Na - 1 - lu;
@@ -174,22 +211,24 @@ __device__ __forceinline__ bool ws_row_setup(const RRArgs& g, const WSShared& S,
 // together, every load of the pass issued before the dependent ones (a
 // mover is often the only warp of the role on its scheduler, so this
 // instruction-level parallelism is its way to hide latency).
-template <int NTH, int NMOV, int RU>
+template <int NTH, int NMOV, int RU, bool BATCH>
 __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S, int tid, int warp, int lane,
                                               int mtid, int mwarp) {
   constexpr int NB = WS_NB;
   constexpr int MTH = NMOV * 32;   // mover threads
   constexpr int MPASS = MTH / NB;  // link rows per mover pass (threads over the NB columns)
-  const csffci_sigma_job_t& sjob = g.job0;
   const int ds = g.ds, LS = g.ls;
   const size_t dsz = (size_t)g.nd_rows * ds, lsz = (size_t)NB * LS;
   const int jl = mtid % NB, ml = mtid / NB;
   int par = 0;
   unsigned mphase = 0;  // parity to wait for next, per stage (bulk copies)
   for (long long u = blockIdx.x; u < g.total_units; u += gridDim.x) {
-    const long long lu = u - sjob.unit_begin;
+    const WSUnit un = ws_unit(g, u);
+    if (BATCH && !ws_batch_job<NTH>(g, S, un.ru, tid)) continue;
+    const csffci_sigma_job_t& sjob = BATCH ? *S.job : g.job0;
+    const long long lu = un.ru - sjob.unit_begin;
     for (int w = 0; w < (sjob.sym ? 2 : 1); ++w) {
-      if (!ws_row_setup<NTH, NB>(g, S, lu, w, par, tid, warp, lane)) break;
+      if (!ws_row_setup<NTH, NB>(g, S, sjob, lu, un.part, un.parts, w, par, tid, warp, lane)) break;
       par ^= 1;
       cp_async_wait_all();
       ws_bar_sync(9, NTH);

@@ -86,6 +86,8 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
   S.srow = &srow;
   S.apoff = (long long*)(smraw + g.off_ap);
   S.mbar = (unsigned long long*)(smraw + g.off_mbar);
+  S.job = nullptr;  // one problem: the job is g.job0
+  S.jst = nullptr;
   // tail partial sums: [tile parity][n-tile][64 doubles]
   double* const Pbuf = (double*)(smraw + g.off_extra);
   const csffci_sigma_job_t& sjob = g.job0;
@@ -116,9 +118,10 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
     bool fresh = true;
     int par = 0;
     for (long long u = blockIdx.x; u < g.total_units; u += gridDim.x) {
-      const long long lu = u - sjob.unit_begin;
+      const WSUnit un = ws_unit(g, u);
+      const long long lu = un.ru - sjob.unit_begin;
       for (int w = 0; w < (sjob.sym ? 2 : 1); ++w) {
-        if (!ws_row_setup<WSR_NTH, NB>(g, S, lu, w, par, tid, warp, lane)) break;
+        if (!ws_row_setup<WSR_NTH, NB>(g, S, sjob, lu, un.part, un.parts, w, par, tid, warp, lane)) break;
         {
           // sign columns of A where this row's alpha sign differs from the
           // one the registers carry
@@ -207,9 +210,10 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
     int par = 0;
     int tpar = 0;  // parity of the tile count (Pbuf half)
     for (long long u = blockIdx.x; u < g.total_units; u += gridDim.x) {
-      const long long lu = u - sjob.unit_begin;
+      const WSUnit un = ws_unit(g, u);
+      const long long lu = un.ru - sjob.unit_begin;
       for (int w = 0; w < (sjob.sym ? 2 : 1); ++w) {
-        if (!ws_row_setup<WSR_NTH, NB>(g, S, lu, w, par, tid, warp, lane)) break;
+        if (!ws_row_setup<WSR_NTH, NB>(g, S, sjob, lu, un.part, un.parts, w, par, tid, warp, lane)) break;
         {
           const unsigned* pcur = S.pneg + par * npair;
           const unsigned* pold = S.pneg + (par ^ 1) * npair;
@@ -266,7 +270,7 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
   } else {
     wsr_reg_dec<WSR_REG_MOV>();
     const int mw = warp - WSR_NBIG - WSR_NTAIL;
-    ws_mover_role<WSR_NTH, WSR_NMOV, WSR_RU>(g, S, tid, warp, lane, mw * 32 + lane, mw);
+    ws_mover_role<WSR_NTH, WSR_NMOV, WSR_RU, false>(g, S, tid, warp, lane, mw * 32 + lane, mw);
   }
 }
 

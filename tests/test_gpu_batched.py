@@ -50,13 +50,53 @@ def test_sigma_many_matches_single_and_oracle():
         np.testing.assert_allclose(out.cpu().numpy(), ref, atol=1e-9)    # sigma tolerance 1e-9
 
 
+def test_sigma_many_warp_specialised_job_table(monkeypatch):
+    """The warp-specialised kernel over a job table (tile variant 4, 8..16
+    orbitals; the default at 10..12 and 14..16, and an autotuner candidate):
+    jobs of mixed electron counts and symmetric / general / antisymmetric
+    modes, several orbital counts, against the one-problem kernel and the
+    oracle."""
+    from pyscf_forge_b200 import batched as B
+    from pyscf_forge_b200.fci import direct_spin1 as D
+    rng = np.random.default_rng(11)
+    cases = [(8, (4, 4), 1), (8, (4, 3), None), (8, (1, 0), None), (9, (5, 4), None), (9, (4, 4), -1),
+             (10, (5, 5), 1), (10, (4, 3), None), (11, (6, 5), None), (11, (5, 5), 1), (12, (6, 6), 1),
+             (12, (7, 6), None), (12, (5, 5), None), (12, (6, 6), -1), (12, (2, 1), None),
+             (13, (6, 5), None), (14, (5, 5), 1), (16, (3, 3), 1), (16, (3, 2), None)]
+    items, host = [], []
+    for norb, nelec, eta in cases:
+        h1, eri = seeded_integrals(norb, 2 * norb, seed=norb * 7 + nelec[0] - nelec[1])
+        h2e = _h2e(h1, eri, norb, nelec)
+        c = rng.standard_normal((comb(norb, nelec[0]), comb(norb, nelec[1])))
+        if eta is not None:
+            c = c + eta * c.T
+        items.append((h2e, torch.as_tensor(c.ravel(), device="cuda"), norb, nelec, eta))
+        host.append((h1, eri, c))
+    monkeypatch.setenv("CSFFCI_SIGMA_VARIANT", "4")
+    outs = B.sigma_many(items)
+    monkeypatch.delenv("CSFFCI_SIGMA_VARIANT")
+    for (h2e, cd, norb, nelec, eta), out, (h1, eri, c) in zip(items, outs, host):
+        one = D.dev_contract_2e(h2e, cd, norb, nelec, eta=eta)
+        np.testing.assert_allclose(out.cpu().numpy(), one.cpu().numpy(), atol=1e-11)
+        if norb <= 10:
+            h2e_np = restate.absorb_h1e(h1, eri, norb, nelec, 0.5)
+            ref = restate.contract_2e(h2e_np, c, norb, nelec).ravel()
+            np.testing.assert_allclose(out.cpu().numpy(), ref, atol=1e-9)    # sigma tolerance 1e-9
+        elif gasref.available() and c.size <= 4_000_000:
+            ref = gasref.contract_2e(restate.absorb_h1e(h1, eri, norb, nelec, 0.5), c, norb, nelec).ravel()
+            np.testing.assert_allclose(out.cpu().numpy(), ref, atol=1e-9)
+
+
 def test_transform_many_round_trip():
     """Batched csf->det and det->csf against the per-transformer kernels for
-    several spaces at once; det->csf(csf->det(x)) == x."""
+    several spaces at once; det->csf(csf->det(x)) == x.  Blocks of at most
+    16 CSFs and 256 determinants take the row-per-thread path, the others
+    (norb 10 and 11 below) the 32 x 32 tiles."""
     from pyscf_forge_b200 import batched as B
     from pyscf_forge_b200.csf_fci.csfstring import CSFTransformer
     rng = np.random.default_rng(9)
-    spaces = [(6, 3, 3, 1), (6, 3, 3, 3), (7, 4, 3, 2), (8, 4, 4, 5), (5, 1, 0, 2), (8, 3, 3, 1)]
+    spaces = [(6, 3, 3, 1), (6, 3, 3, 3), (7, 4, 3, 2), (8, 4, 4, 5), (5, 1, 0, 2), (8, 3, 3, 1),
+              (10, 5, 5, 1), (11, 6, 5, 2), (12, 6, 6, 3)]
     ts = [CSFTransformer(*s) for s in spaces]
     xs = [torch.as_tensor(rng.standard_normal((1 + i % 3, t.ncsf)), device="cuda") for i, t in enumerate(ts)]
     dets = B.transform_many(list(zip(ts, xs)), reverse=True)
@@ -113,8 +153,27 @@ def test_device_engine_matches_host_engine_and_graph_replay():
         assert a[3] and b[3] and c[3]
         np.testing.assert_allclose(a[0], b[0], atol=1e-10)
         np.testing.assert_allclose(a[0], c[0], atol=1e-10)
-    assert sg.tile_variants and all(0 <= v < 4 for v in sg.tile_variants.values())
+    assert sg.tile_variants and all(0 <= v <= 4 for v in sg.tile_variants.values())
     assert set(sg.tile_variants) <= {p.norb for p in probs}
+
+
+def test_device_engine_warp_specialised_gated(monkeypatch):
+    """The device-resident plan with every orbital count from 8 up on the
+    warp-specialised job-table kernel (autotuner off, variant 4 named):
+    its jobs are gated as problems converge, so units of converged problems
+    are skipped inside the launch.  Same energies as the tile-shape kernel."""
+    from pyscf_forge_b200 import batched as B
+    probs = B.make_uneven_batch(12, seed0=3100, norb_lo=8, norb_hi=11)
+    kw = dict(conv_tol=1e-12, conv_tol_residual=1e-7, max_cycle=400)
+    ref = B.BatchedCSFSolver(engine="device", autotune=False, **kw).kernel(probs, with_rdm=False)
+    monkeypatch.setenv("CSFFCI_SIGMA_VARIANT", "4")
+    sw = B.BatchedCSFSolver(engine="device", autotune=False, **kw)
+    got = sw.kernel(probs, with_rdm=False)
+    monkeypatch.delenv("CSFFCI_SIGMA_VARIANT")
+    for p, a, b in zip(probs, got, ref):
+        assert a[3] and b[3]
+        np.testing.assert_allclose(a[0], b[0], atol=1e-10)
+    assert all(v == 4 for n, v in sw.tile_variants.items() if n >= 8)
 
 
 def test_c3_batch_energies_vs_reference():

@@ -18,11 +18,26 @@ import random
 import pytest
 
 
-def _mma_warp(rows, tail=None):
+def _job_lookups(rows):
+    """A job-table launch (batch=True) looks up each unit's job first
+    (ws_batch_job: two barrier-9 syncs); a gated unit (None) stops there.
+    Yields None before each lookup and the tile count of each row."""
+    for r in rows:
+        yield None
+        if r is not None:
+            yield from (r if isinstance(r, tuple) else (r,))
+
+
+def _mma_warp(rows, tail=None, batch=False):
     """tail: None for an MMA warp without partial sums, else (n-tile, K
     half) of a tail warp of the register-split kernel."""
     t = 0  # tiles so far (its parity indexes the partial-sum buffer)
-    for r, nch in enumerate(rows):
+    seq = _job_lookups(rows) if batch else rows
+    for r, nch in enumerate(seq):
+        if nch is None:
+            yield ("sync", 9, None)
+            yield ("sync", 9, None)
+            continue
         for _ in range(4):  # ws_row_setup (3) + after the fold (1)
             yield ("sync", 9, None)
         for c in range(nch):
@@ -37,8 +52,12 @@ def _mma_warp(rows, tail=None):
             t += 1
 
 
-def _mover_warp(rows):
-    for nch in rows:
+def _mover_warp(rows, batch=False):
+    for nch in (_job_lookups(rows) if batch else rows):
+        if nch is None:
+            yield ("sync", 9, None)
+            yield ("sync", 9, None)
+            continue
         for _ in range(4):
             yield ("sync", 9, None)
         for c in range(nch + 2):
@@ -50,13 +69,13 @@ def _mover_warp(rows):
                 yield ("sync", 4 + (c - 2) % 3, ("V", c - 2))
 
 
-def _run(rows, nwm, nmov, seed, tails=()):
+def _run(rows, nwm, nmov, seed, tails=(), batch=False):
     rng = random.Random(seed)
     counts = {9: nwm + nmov, 7: nmov, 8: nwm}
     for s in range(3):
         counts[1 + s] = counts[4 + s] = nwm + nmov
-    warps = ([_mma_warp(rows) for _ in range(nwm - len(tails))] + [_mma_warp(rows, t) for t in tails]
-             + [_mover_warp(rows) for _ in range(nmov)])
+    warps = ([_mma_warp(rows, batch=batch) for _ in range(nwm - len(tails))]
+             + [_mma_warp(rows, t, batch) for t in tails] + [_mover_warp(rows, batch) for _ in range(nmov)])
     slots = {}
     cur = [next(w) for w in warps]
     blocked, gen = {}, {b: 0 for b in counts}
@@ -114,3 +133,15 @@ def test_wsr_tail_partial_sums():
     for rows in ([1], [2], [3], [1, 4, 2, 7, 3], [5, 1, 1, 6], [10, 9, 8]):
         for seed in range(40):
             _run(rows, 12, 4, seed, tails)
+
+
+@pytest.mark.parametrize("nwm,nmov", [(5, 3), (8, 4), (7, 5), (9, 3), (12, 4)])
+def test_ws_job_table_protocol(nwm, nmov):
+    """The job-table form at 8..12 orbitals (MMA warps, movers as the kernel
+    lays them out): units of live jobs with one row or a spin-symmetric pair
+    of rows (a tuple), and gated units (None) that only look up their job."""
+    units = ([None], [3, None, 2], [(2, 5), None, None, 4], [None, (1, 0), 6, None, (3, 3)],
+             [0, None, (0, 2), 1], [4, 4, None, 4, (7, 1)])
+    for rows in units:
+        for seed in range(25):
+            _run(rows, nwm, nmov, seed, batch=True)
