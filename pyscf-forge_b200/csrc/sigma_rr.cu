@@ -54,7 +54,8 @@ static const int kVariantShape[RR_NVARIANT][2] = {{16, 4}, {8, 4}, {16, 2}, {8, 
 bool rr_variant_valid(int norb, int v) { return v >= 0 && v < RR_NVARIANT && !(v == 0 && norb >= 15); }
 
 bool batch_variant_valid(int norb, int v) {
-  return rr_variant_valid(norb, v) || (v == RR_VARIANT_WS && sigma_ws_supported(norb));
+  return rr_variant_valid(norb, v) || (v == RR_VARIANT_WS && sigma_ws_supported(norb)) ||
+         (v == RR_VARIANT_WS16 && sigma_ws16_supported(norb));
 }
 
 // one problem: the register-split kernel at 16 orbitals, else the job-table
@@ -63,7 +64,7 @@ int sigma_rr_single_variant(int norb) {
   const char* env = getenv("CSFFCI_SIGMA_VARIANT");
   if (env) {
     const int v = atoi(env);
-    if (v == RR_VARIANT_WS && sigma_ws_supported(norb)) return RR_VARIANT_WS;
+    if (batch_variant_valid(norb, v)) return v;
     if ((v == RR_VARIANT_WSR || v == RR_VARIANT_WSR_BULK) && sigma_wsr_supported(norb)) return v;
     if (rr_variant_valid(norb, v)) return v;
   }
@@ -126,8 +127,9 @@ int sigma_rr_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev,
   const int ks = (npair + 3) / 4;
   if (variant < 0 && !jobs_dev) variant = sigma_rr_single_variant(norb);
   if (variant < 0) variant = rr_default_variant(norb);
-  if (variant == RR_VARIANT_WS)
-    return sigma_ws_launch(norb, njobs, jobs_dev, job0, total_units, max_nb, max_nla, max_nlb, stream);
+  if (variant == RR_VARIANT_WS || variant == RR_VARIANT_WS16)
+    return sigma_ws_launch(norb, njobs, jobs_dev, job0, total_units, max_nb, max_nla, max_nlb, stream,
+                           variant == RR_VARIANT_WS16 ? 16 : 8);
   if (variant == RR_VARIANT_WSR || variant == RR_VARIANT_WSR_BULK) {
     if (jobs_dev) {
       set_error("sigma: the register-split variant takes one problem, not a job table");
@@ -330,7 +332,7 @@ int sigma_batch_tune(SigmaBatchInfo& info, const csffci_sigma_job_t* jobs_host, 
   CSF_CUDA(cudaEventCreate(&b));
   int best = rr_default_variant(info.norb);
   float best_ms = 1e30f;
-  for (int v = 0; v <= RR_VARIANT_WS; ++v) {
+  for (int v = 0; v <= RR_VARIANT_WS16; ++v) {
     if (!batch_variant_valid(info.norb, v)) continue;
     SigmaBatchInfo t = info;
     t.variant = v;

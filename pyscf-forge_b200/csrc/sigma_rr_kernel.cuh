@@ -420,11 +420,15 @@ static int launch_rr(RRArgs& g, size_t smem, cudaStream_t stream) {
 // tile-shape variants: (rows per warp, n-tiles of 8 columns)
 constexpr int RR_NVARIANT = 4;
 // the warp-specialised kernel (sigma_ws.cu), 8..16 orbitals, one problem
-// or a job table
+// or a job table: one MMA warp per 8 rows (variant 4) or, up to 12
+// orbitals, per 16 rows in CTAs of 8 warps (variant 7)
 constexpr int RR_VARIANT_WS = 4;
+constexpr int RR_VARIANT_WS16 = 7;
 bool sigma_ws_supported(int norb);
+bool sigma_ws16_supported(int norb);
 int sigma_ws_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev, const csffci_sigma_job_t& job0,
-                    long long total_units, long long max_nb, int max_nla, int max_nlb, cudaStream_t stream);
+                    long long total_units, long long max_nb, int max_nla, int max_nlb, cudaStream_t stream,
+                    int mw);
 // the warp-specialised kernel with registers re-split between the roles
 // (sigma_wsr.cu), one problem at 16 orbitals
 constexpr int RR_VARIANT_WSR = 5;

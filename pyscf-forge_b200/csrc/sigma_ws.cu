@@ -38,7 +38,7 @@ namespace csffci {
 // MMA warps: one per m-tile of 8 rows, the last m-tiles split over two warps
 // (one n-tile each) when MT mod 4 is 1 or 2; movers fill the CTA to a
 // multiple of four warps with at least two.
-template <int MT>
+template <int MT, int MW = 8>
 struct WSLayout {
   static constexpr int q = MT / 4, r = MT % 4;
   // splitting balances the MMA units over the schedulers; it is skipped
@@ -46,17 +46,18 @@ struct WSLayout {
   // and 2 movers against 17 and 3), the movers being the limit there
   static constexpr bool split0 = q >= 1 && (r == 1 || r == 2);
   static constexpr int NWM0 = split0 ? 4 * q + 2 * r : MT;
-  static constexpr bool split = split0 && 4 * ((NWM0 + 2 + 3) / 4) - NWM0 >= 3;
+  static constexpr bool split = MW == 8 && split0 && 4 * ((NWM0 + 2 + 3) / 4) - NWM0 >= 3;
   static constexpr int NWM = split ? NWM0 : MT;
-  static constexpr int NTOT = 4 * ((NWM + 2 + 3) / 4);
+  // 16-row MMA warps (up to 12 orbitals): at least three movers
+  static constexpr int NTOT = MW == 8 ? 4 * ((NWM + 2 + 3) / 4) : 4 * ((NWM + 3 + 3) / 4);
   static constexpr int NMOV = NTOT - NWM;
 };
 
 constexpr int WS_RU = 4;      // links a mover thread handles together (loads in flight)
 
-template <int KS, int MT, bool BATCH, int MINB>
-__global__ void __launch_bounds__(WSLayout<MT>::NTOT * 32, MINB) k_sigma_ws(RRArgs g) {
-  using L = WSLayout<MT>;
+template <int KS, int MT, int MW, bool BATCH, int MINB>
+__global__ void __launch_bounds__(WSLayout<MT, MW>::NTOT * 32, MINB) k_sigma_ws(RRArgs g) {
+  using L = WSLayout<MT, MW>;
   constexpr int NB = WS_NB;
   constexpr int NTH = L::NTOT * 32;
   constexpr int NWM = L::NWM, NMOV = L::NMOV;
@@ -96,14 +97,15 @@ __global__ void __launch_bounds__(WSLayout<MT>::NTOT * 32, MINB) k_sigma_ws(RRAr
     const bool part = L::split && warp >= 4 * L::q;
     const int mt = part ? 4 * L::q + (warp - 4 * L::q) / 2 : warp;
     const int t0 = part ? (warp - 4 * L::q) % 2 : 0;
-    double a0f[KS];
-    // h2e rows 8 mt + g of the job, columns 4k + t (without signs)
+    double a0f[KS], a1f[MW == 16 ? KS : 1];
+    // h2e rows MW mt + g (and + 8) of the job, columns 4k + t (without signs)
     auto load_a = [&](const double* h2e) {
-      const int r0 = mt * 8 + gq;
+      const int r0 = mt * MW + gq, r1 = r0 + 8;
 #pragma unroll
       for (int k = 0; k < KS; ++k) {
         const int c = 4 * k + tq;
         a0f[k] = (r0 < npair && c < npair) ? h2e[(long long)r0 * npair + c] : 0.0;
+        if (MW == 16) a1f[k] = (r1 < npair && c < npair) ? h2e[(long long)r1 * npair + c] : 0.0;
       }
     };
     if (!BATCH) load_a(g.job0.h2e);
@@ -132,7 +134,10 @@ __global__ void __launch_bounds__(WSLayout<MT>::NTOT * 32, MINB) k_sigma_ws(RRAr
 #pragma unroll
           for (int k = 0; k < KS; ++k) {
             const int c = 4 * k + tq;
-            if (c < npair && ((fresh ? 0u : pold[c]) ^ pcur[c])) a0f[k] = -a0f[k];
+            if (c < npair && ((fresh ? 0u : pold[c]) ^ pcur[c])) {
+              a0f[k] = -a0f[k];
+              if (MW == 16) a1f[k] = -a1f[k];
+            }
           }
         }
         fresh = false;
@@ -143,6 +148,53 @@ __global__ void __launch_bounds__(WSLayout<MT>::NTOT * 32, MINB) k_sigma_ws(RRAr
         for (int c = 0; c < nch; ++c) {
           const int s = c % WS_STAGES;
           ws_bar_sync(1 + s, NTH);  // D of tile c is gathered
+          if constexpr (MW == 16) {
+            // rows r0 = 16 mt + g and r1 = r0 + 8, both n-tiles (m16n8k4)
+            double acc[2][4];
+#pragma unroll
+            for (int t = 0; t < 2; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.0;
+            const double* Db = S.Dbuf + s * dsz + tq * ds + gq;
+#pragma unroll
+            for (int k = 0; k < KS; ++k) {
+              rr_dmma16(acc[0], a0f[k], a1f[k], Db[4 * k * ds]);
+              rr_dmma16(acc[1], a0f[k], a1f[k], Db[4 * k * ds + 8]);
+            }
+            ws_bar_sync(8, NWM * 32);  // every MMA warp has read D of tile c
+            const int r0 = mt * 16 + gq, r1 = r0 + 8;
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+              if (r0 < npair) {
+                double* V = S.Dbuf + s * dsz + r0 * ds + 8 * t + 2 * tq;
+                V[0] = acc[t][0];
+                V[1] = acc[t][1];
+              }
+              if (r1 < npair) {
+                double* V = S.Dbuf + s * dsz + r1 * ds + 8 * t + 2 * tq;
+                V[0] = acc[t][2];
+                V[1] = acc[t][3];
+              }
+            }
+            ws_bar_arrive(4 + s, NTH);  // V of tile c is written
+            // the alpha scatter of this lane's two pair rows (as below)
+            double* const obase = sjob.sym ? sjob.scratch : sjob.sigma;
+            const int alim = (int)(sjob.sym ? srow.ja : sjob.Nb);
+            const int J = (srow.c0 + c) * NB + 2 * tq;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int r = h ? r1 : r0;
+              const long long aoff = r < npair ? S.apoff[r] : -1;
+              if (aoff >= 0) {
+                double* const abase = obase + aoff;
+                const unsigned aneg = S.pneg[srow.pc + r];
+#pragma unroll
+                for (int t = 0; t < 2; ++t) {
+                  if (J + 8 * t < alim) atomicAdd(abase + J + 8 * t, rr_flip(acc[t][2 * h], aneg));
+                  if (J + 8 * t + 1 < alim) atomicAdd(abase + J + 8 * t + 1, rr_flip(acc[t][2 * h + 1], aneg));
+                }
+              }
+            }
+            continue;
+          }
           double acc[2][2];
           acc[0][0] = acc[0][1] = acc[1][0] = acc[1][1] = 0.0;
           const double* Db = S.Dbuf + s * dsz + tq * ds + gq + 8 * t0;
@@ -195,17 +247,19 @@ __global__ void __launch_bounds__(WSLayout<MT>::NTOT * 32, MINB) k_sigma_ws(RRAr
 }
 
 bool sigma_ws_supported(int norb) { return norb >= 8 && norb <= 16; }
+bool sigma_ws16_supported(int norb) { return norb >= 8 && norb <= 12; }
 
 // CTAs per SM the registers are sized for: below 13 orbitals the A
 // fragments are small enough for two CTAs per SM, so that one CTA's row
 // setup (barrier 9) overlaps the other's tiles
 constexpr int ws_min_blocks(int norb) { return norb <= 12 ? 2 : 1; }
 
-template <int KS, int MT, int NORB>
+template <int KS, int MT, int NORB, int MW>
 static int launch_ws(RRArgs& g, size_t smem, cudaStream_t stream) {
-  constexpr int NTH = WSLayout<MT>::NTOT * 32;
-  constexpr int MINB = ws_min_blocks(NORB);
-  auto kern = g.jobs ? k_sigma_ws<KS, MT, true, MINB> : k_sigma_ws<KS, MT, false, MINB>;
+  constexpr int NTH = WSLayout<MT, MW>::NTOT * 32;
+  // 16-row MMA warps: 8-warp CTAs, three per SM
+  constexpr int MINB = MW == 16 ? 2 : ws_min_blocks(NORB);
+  auto kern = g.jobs ? k_sigma_ws<KS, MT, MW, true, MINB> : k_sigma_ws<KS, MT, MW, false, MINB>;
   CSF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, nsm = 148, per_sm = 0;
   CSF_CUDA(cudaGetDevice(&dev));
@@ -219,10 +273,14 @@ static int launch_ws(RRArgs& g, size_t smem, cudaStream_t stream) {
   ws_split_last_round(g, grid);
   if (grid > g.total_units) grid = g.total_units;
   if (grid < 1) return CSFFCI_OK;
-  static const char* names[17] = {"", "", "", "", "", "", "", "", "k_sigma_ws_n8", "k_sigma_ws_n9",
-                                  "k_sigma_ws_n10", "k_sigma_ws_n11", "k_sigma_ws_n12", "k_sigma_ws_n13",
-                                  "k_sigma_ws_n14", "k_sigma_ws_n15", "k_sigma_ws_n16"};
-  ProfScope ps(g.jobs ? names[NORB] : "k_sigma_ws", stream);
+  static const char* names8[17] = {"", "", "", "", "", "", "", "", "k_sigma_ws_n8", "k_sigma_ws_n9",
+                                   "k_sigma_ws_n10", "k_sigma_ws_n11", "k_sigma_ws_n12", "k_sigma_ws_n13",
+                                   "k_sigma_ws_n14", "k_sigma_ws_n15", "k_sigma_ws_n16"};
+  static const char* names16[13] = {"", "", "", "", "", "", "", "", "k_sigma_ws16_n8", "k_sigma_ws16_n9",
+                                    "k_sigma_ws16_n10", "k_sigma_ws16_n11", "k_sigma_ws16_n12"};
+  const char* name = MW == 16 ? (g.jobs ? names16[NORB <= 12 ? NORB : 0] : "k_sigma_ws16")
+                              : (g.jobs ? names8[NORB] : "k_sigma_ws");
+  ProfScope ps(name, stream);
   kern<<<(int)grid, NTH, smem, stream>>>(g);
   return check_launch("sigma (warp-specialised)");
 }
@@ -258,9 +316,10 @@ size_t ws_layout(RRArgs& g, int npair, int rows_multiple, long long max_nb, int 
 }
 
 int sigma_ws_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev, const csffci_sigma_job_t& job0,
-                    long long total_units, long long max_nb, int max_nla, int max_nlb, cudaStream_t stream) {
-  if (!sigma_ws_supported(norb)) {
-    set_error("sigma: the warp-specialised variant covers norb 8..16, not %d", norb);
+                    long long total_units, long long max_nb, int max_nla, int max_nlb, cudaStream_t stream,
+                    int mw) {
+  if (!(mw == 8 ? sigma_ws_supported(norb) : sigma_ws16_supported(norb))) {
+    set_error("sigma: no warp-specialised kernel with %d-row MMA warps for norb %d", mw, norb);
     return CSFFCI_ERR_INVALID;
   }
   const int npair = norb * (norb + 1) / 2;
@@ -272,21 +331,30 @@ int sigma_ws_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev, con
   g.parts = 1;
   g.split_from = total_units;
   g.total_units = total_units;
-  const size_t smem = ws_layout(g, npair, 8, max_nb, max_nla, max_nlb, 0, nullptr);
+  const size_t smem = ws_layout(g, npair, mw, max_nb, max_nla, max_nlb, 0, nullptr);
   if (smem == 0) {
     set_error("sigma: warp-specialised tiles exceed shared memory (norb %d)", norb);
     return CSFFCI_ERR_INVALID;
   }
+  if (mw == 16) {
+    switch (norb) {  // KS = ceil(npair / 4), MT = ceil(npair / 16)
+      case 8: return launch_ws<9, 3, 8, 16>(g, smem, stream);
+      case 9: return launch_ws<12, 3, 9, 16>(g, smem, stream);
+      case 10: return launch_ws<14, 4, 10, 16>(g, smem, stream);
+      case 11: return launch_ws<17, 5, 11, 16>(g, smem, stream);
+      default: return launch_ws<20, 5, 12, 16>(g, smem, stream);
+    }
+  }
   switch (norb) {  // KS = ceil(npair / 4), MT = ceil(npair / 8)
-    case 8: return launch_ws<9, 5, 8>(g, smem, stream);
-    case 9: return launch_ws<12, 6, 9>(g, smem, stream);
-    case 10: return launch_ws<14, 7, 10>(g, smem, stream);
-    case 11: return launch_ws<17, 9, 11>(g, smem, stream);
-    case 12: return launch_ws<20, 10, 12>(g, smem, stream);
-    case 13: return launch_ws<23, 12, 13>(g, smem, stream);
-    case 14: return launch_ws<27, 14, 14>(g, smem, stream);
-    case 15: return launch_ws<30, 15, 15>(g, smem, stream);
-    default: return launch_ws<34, 17, 16>(g, smem, stream);
+    case 8: return launch_ws<9, 5, 8, 8>(g, smem, stream);
+    case 9: return launch_ws<12, 6, 9, 8>(g, smem, stream);
+    case 10: return launch_ws<14, 7, 10, 8>(g, smem, stream);
+    case 11: return launch_ws<17, 9, 11, 8>(g, smem, stream);
+    case 12: return launch_ws<20, 10, 12, 8>(g, smem, stream);
+    case 13: return launch_ws<23, 12, 13, 8>(g, smem, stream);
+    case 14: return launch_ws<27, 14, 14, 8>(g, smem, stream);
+    case 15: return launch_ws<30, 15, 15, 8>(g, smem, stream);
+    default: return launch_ws<34, 17, 16, 8>(g, smem, stream);
   }
 }
 

@@ -50,9 +50,12 @@ def test_sigma_many_matches_single_and_oracle():
         np.testing.assert_allclose(out.cpu().numpy(), ref, atol=1e-9)    # sigma tolerance 1e-9
 
 
-def test_sigma_many_warp_specialised_job_table(monkeypatch):
-    """The warp-specialised kernel over a job table (tile variant 4, 8..16
-    orbitals; the default at 10..12 and 14..16, and an autotuner candidate):
+@pytest.mark.parametrize("variant", ["4", "7"])
+def test_sigma_many_warp_specialised_job_table(monkeypatch, variant):
+    """The warp-specialised kernel over a job table: variant 4 (8-row MMA
+    warps, 8..16 orbitals; the default at 10..12 and 14..16) and variant 7
+    (16-row MMA warps in 8-warp CTAs, 8..12 orbitals), both autotuner
+    candidates.  Jobs past a variant's orbital range run the default kernel:
     jobs of mixed electron counts and symmetric / general / antisymmetric
     modes, several orbital counts, against the one-problem kernel and the
     oracle."""
@@ -72,7 +75,7 @@ def test_sigma_many_warp_specialised_job_table(monkeypatch):
             c = c + eta * c.T
         items.append((h2e, torch.as_tensor(c.ravel(), device="cuda"), norb, nelec, eta))
         host.append((h1, eri, c))
-    monkeypatch.setenv("CSFFCI_SIGMA_VARIANT", "4")
+    monkeypatch.setenv("CSFFCI_SIGMA_VARIANT", variant)
     outs = B.sigma_many(items)
     monkeypatch.delenv("CSFFCI_SIGMA_VARIANT")
     for (h2e, cd, norb, nelec, eta), out, (h1, eri, c) in zip(items, outs, host):
@@ -153,27 +156,30 @@ def test_device_engine_matches_host_engine_and_graph_replay():
         assert a[3] and b[3] and c[3]
         np.testing.assert_allclose(a[0], b[0], atol=1e-10)
         np.testing.assert_allclose(a[0], c[0], atol=1e-10)
-    assert sg.tile_variants and all(0 <= v <= 4 for v in sg.tile_variants.values())
+    assert sg.tile_variants and all(0 <= v <= 4 or v == 7 for v in sg.tile_variants.values())
     assert set(sg.tile_variants) <= {p.norb for p in probs}
 
 
-def test_device_engine_warp_specialised_gated(monkeypatch):
-    """The device-resident plan with every orbital count from 8 up on the
-    warp-specialised job-table kernel (autotuner off, variant 4 named):
+@pytest.mark.parametrize("variant", ["4", "7"])
+def test_device_engine_warp_specialised_gated(monkeypatch, variant):
+    """The device-resident plan with every orbital count from 8 up on a
+    warp-specialised job-table kernel (autotuner off, the variant named):
     its jobs are gated as problems converge, so units of converged problems
-    are skipped inside the launch.  Same energies as the tile-shape kernel."""
+    are skipped inside the launch.  Same energies as the tile-shape kernel
+    (variant 2)."""
     from pyscf_forge_b200 import batched as B
     probs = B.make_uneven_batch(12, seed0=3100, norb_lo=8, norb_hi=11)
     kw = dict(conv_tol=1e-12, conv_tol_residual=1e-7, max_cycle=400)
+    monkeypatch.setenv("CSFFCI_SIGMA_VARIANT", "2")
     ref = B.BatchedCSFSolver(engine="device", autotune=False, **kw).kernel(probs, with_rdm=False)
-    monkeypatch.setenv("CSFFCI_SIGMA_VARIANT", "4")
+    monkeypatch.setenv("CSFFCI_SIGMA_VARIANT", variant)
     sw = B.BatchedCSFSolver(engine="device", autotune=False, **kw)
     got = sw.kernel(probs, with_rdm=False)
     monkeypatch.delenv("CSFFCI_SIGMA_VARIANT")
     for p, a, b in zip(probs, got, ref):
         assert a[3] and b[3]
         np.testing.assert_allclose(a[0], b[0], atol=1e-10)
-    assert all(v == 4 for n, v in sw.tile_variants.items() if n >= 8)
+    assert all(v == int(variant) for n, v in sw.tile_variants.items() if 8 <= n <= 12)
 
 
 def test_c3_batch_energies_vs_reference():
