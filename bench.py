@@ -610,6 +610,57 @@ def run_batched(nprob):
                        "e2e": "host integrals in, host energies/CI/RDMs out (both forms)"}}
 
 
+def run_batch_sigma(norbs, variants, steps=3):
+    """Per-launch time of the batched sigma (csffci_sigma_batch) of the C3
+    problems of the given orbital counts, one job per root with a seeded
+    random vector (symmetrised for equal electron counts, as the solver's
+    vectors are), for each sigma kernel variant (CSFFCI_SIGMA_VARIANT)."""
+    import numpy as np
+    import torch
+    from math import comb
+    from pyscf_forge_b200 import _capi
+    from pyscf_forge_b200 import batched as Bt
+    from pyscf_forge_b200.fci import direct_spin1 as D
+    from pyscf_forge_b200._runtime import eri_pair_matrix
+    rng = np.random.default_rng(1)
+    items = []
+    for p in Bt.make_uneven_batch(128):
+        if p.norb not in norbs:
+            continue
+        na, nb = comb(p.norb, p.nelec[0]), comb(p.norb, p.nelec[1])
+        h2e = D.dev_absorb_h1e(p.h1, eri_pair_matrix(p.eri, p.norb), p.norb, p.nelec, 0.5)
+        eta = (-1 if p.smult == 3 else 1) if p.nelec[0] == p.nelec[1] else None
+        for _ in range(p.nroots):
+            c = rng.standard_normal((na, nb))
+            if eta is not None:
+                c = c + eta * c.T
+            items.append((h2e, torch.as_tensor(c.ravel(), device="cuda"), p.norb, p.nelec, eta))
+    old = os.environ.get("CSFFCI_SIGMA_VARIANT")
+    out = {"workload": "C3 batch, norb %s: %d jobs (one per root)" % (sorted(norbs), len(items)), "variants": {}}
+    ref = None
+    try:
+        for v in variants:
+            os.environ["CSFFCI_SIGMA_VARIANT"] = str(v)
+            res = Bt.sigma_many(items)  # warm-up (and the result to compare)
+            if ref is None:
+                ref = [r.clone() for r in res]
+            err = max(float((a - b).abs().max()) for a, b in zip(res, ref))
+            _capi.profile_enable(True)
+            for _ in range(steps):
+                Bt.sigma_many(items)
+            prof = _capi.profile_report()
+            _capi.profile_enable(False)
+            out["variants"][str(v)] = {"max_abs_diff_vs_first": err,
+                                       "ms_per_launch": {k: round(t[1] / t[0], 3) for k, t in sorted(prof.items())
+                                                         if "sigma" in k}}
+    finally:
+        if old is None:
+            os.environ.pop("CSFFCI_SIGMA_VARIANT", None)
+        else:
+            os.environ["CSFFCI_SIGMA_VARIANT"] = old
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -630,6 +681,9 @@ def main():
     ap.add_argument("--rdm-only", default="", help="only the RDM timing of these cases "
                     "(cas16_singlet_1root,cas14_sa2), for profiling captures")
     ap.add_argument("--batch", type=int, default=128, help="problems in the batched-solves measurement")
+    ap.add_argument("--batch-sigma-only", default="", help="only the batched sigma launches of the C3 "
+                    "problems of these orbital counts (e.g. 10,11,12), per kernel variant")
+    ap.add_argument("--sigma-variants", default="0,1,2,3,4,7", help="variants for --batch-sigma-only")
     args = ap.parse_args()
     global C4_MAX_CYCLE
     if args.c4_max_cycle:
@@ -650,6 +704,13 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         if rank == 0:
             print(json.dumps(run_c4(ref_check=not args.no_cpu_baseline)), flush=True)
+        return
+    if args.batch_sigma_only:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        if rank == 0:
+            print(json.dumps(run_batch_sigma({int(x) for x in args.batch_sigma_only.split(",")},
+                                             [int(x) for x in args.sigma_variants.split(",")])), flush=True)
         return
     if args.rdm_only:
         # the adjoint timing alone (profiling captures of the RDM kernels)
