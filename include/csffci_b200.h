@@ -209,8 +209,19 @@ enum {
   CSFFCI_SIGMA_SPIN_SYMMETRIC = 2, /* ci == eta * ci^T (na == nb): only the
                                       Jb <= Ja half of the contraction is
                                       formed, then sigma = s + eta * s^T */
-  CSFFCI_SIGMA_REFERENCE_KERNEL = 4 /* force the simple shared-memory-h2e
-                                       kernel (used to cross-check) */
+  CSFFCI_SIGMA_REFERENCE_KERNEL = 4, /* force the simple shared-memory-h2e
+                                        kernel (used to cross-check) */
+  CSFFCI_SIGMA_DETERMINISTIC = 8 /* bit-identical reruns (8 <= norb <= 16):
+                                    every scattered contribution is split
+                                    into three fixed-point digits (weights
+                                    2^-80, 2^-37, 2^6) added by 64-bit
+                                    integer atomics, whose order does not
+                                    change the sums; sigma is formed from
+                                    the digit sums afterwards.  Workspace:
+                                    3 * ndet int64; contributions must stay
+                                    below 2^55 in magnitude.  No counterpart
+                                    in the reference (its CPU sigma runs in
+                                    a fixed order per thread count). */
 };
 
 size_t csffci_sigma_workspace(int norb, int neleca, int nelecb, int flags);
@@ -233,7 +244,8 @@ int csffci_sigma(int norb, int neleca, int nelecb, const double* h2e,
  * (device pointers that must outlive the plan; their contents are read at
  * every execute), fixes the sigma kernel for (norb, neleca, nelecb) and
  * returns the workspace the plan needs (the spin-symmetric scratch when
- * flags holds CSFFCI_SIGMA_SPIN_SYMMETRIC; flags may also hold
+ * flags holds CSFFCI_SIGMA_SPIN_SYMMETRIC, the three digit planes with
+ * CSFFCI_SIGMA_DETERMINISTIC; flags may also hold
  * CSFFCI_SIGMA_REFERENCE_KERNEL).  bind hands that workspace over (caller
  * owned, for the life of the plan).  execute computes sigma from ci on the
  * stream, with flags ACCUMULATE and/or SPIN_SYMMETRIC (the latter only
@@ -249,8 +261,8 @@ int csffci_sigma_plan_create(int norb, int neleca, int nelecb, const double* h2e
 int csffci_sigma_plan_bind(csffci_sigma_plan_t* plan, void* work, size_t work_bytes);
 int csffci_sigma_plan_execute(const csffci_sigma_plan_t* plan, const double* ci, double* sigma, int eta,
                               int flags, cudaStream_t stream);
-/* the kernel the plan runs: 0..3 register-resident tile variants, 4 and 5
- * the warp-specialised kernels, -2 the shared-memory-h2e kernel */
+/* the kernel the plan runs: 0..3 register-resident tile variants, 4, 5
+ * and 7 the warp-specialised kernels, -2 the shared-memory-h2e kernel */
 int csffci_sigma_plan_variant(const csffci_sigma_plan_t* plan);
 void csffci_sigma_plan_destroy(csffci_sigma_plan_t* plan);
 

@@ -18,6 +18,7 @@ CSFFCI_ERR_TIMEOUT = -4
 SIGMA_ACCUMULATE = 1
 SIGMA_SPIN_SYMMETRIC = 2
 SIGMA_REFERENCE_KERNEL = 4
+SIGMA_DETERMINISTIC = 8
 
 
 class LinkEntry(ctypes.Structure):

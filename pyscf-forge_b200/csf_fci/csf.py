@@ -186,13 +186,14 @@ class _Hop:
     """x (k, ncsf) -> H x in the CSF basis:
     csf2det -> sigma (+ spin part of h1e) -> det2csf (csf.py:447-450)."""
 
-    def __init__(self, transformer, h2eff, norb, nelec):
+    def __init__(self, transformer, h2eff, norb, nelec, deterministic=False):
         self.t = transformer
         self.h2e = h2eff.h2e
         self.h1e_s = h2eff.h1e_s
         self.norb = norb
         self.nelec = nelec
         self.eta = transformer.spin_parity
+        self.deterministic = bool(deterministic)
         self.nsigma = 0
 
     def __call__(self, x):
@@ -201,7 +202,7 @@ class _Hop:
         hx = torch.empty_like(xd)
         for i in range(xd.shape[0]):
             direct_spin1.dev_contract_2e(self.h2e, xd[i], self.norb, self.nelec, eta=self.eta,
-                                         out=hx[i])
+                                         out=hx[i], deterministic=self.deterministic)
             if self.h1e_s is not None:
                 direct_spin1.dev_contract_1e(self.h1e_s, -self.h1e_s, xd[i], self.norb, self.nelec,
                                              hx[i])
@@ -274,7 +275,7 @@ def kernel(fci, h1e, eri, norb, nelec, smult=None, idx_sym=None, ci0=None, tol=N
     h2e = fci.absorb_h1e(h1e, eri, norb, nelec, .5)
     if not isinstance(h2e, H2eff):
         h2e = H2eff(to_dev(eri_pair_matrix(h2e, norb)))
-    hop = _Hop(transformer, h2e, norb, nelec)
+    hop = _Hop(transformer, h2e, norb, nelec, deterministic=getattr(fci, 'deterministic_sigma', False))
 
     if ci0 is None:
         x0 = get_init_guess(norb, nelec, nroots, hdiag_csf, transformer)
@@ -398,11 +399,16 @@ class CSFFCISolver:
     gas_restr_type as the reference's GAS solver takes them,
     pyscf/mcscf/fci_gas.py:778-801; the restriction has to be spin
     complete, see csf_fci.gas)."""
-    _keys = {'smult', 'transformer', 'gas_orbs', 'gas_restr', 'gas_restr_type'}
+    _keys = {'smult', 'transformer', 'gas_orbs', 'gas_restr', 'gas_restr_type', 'deterministic_sigma'}
     pspace_size = 200
     gas_orbs = None
     gas_restr = None
     gas_restr_type = _gas.GAS_RESTR_SPIN_SUPERGROUP
+    # sigma with the deterministic scatter (CSFFCI_SIGMA_DETERMINISTIC,
+    # 8 <= norb <= 16): reruns give bit-identical sigma vectors, energies
+    # and CI vectors, at the cost of three integer atomics per scattered
+    # element; the solve then takes the host-driven Davidson loop
+    deterministic_sigma = False
 
     def __init__(self, mol=None, smult=None):
         self.smult = smult
@@ -459,7 +465,8 @@ class CSFFCISolver:
         if nelec[0] == nelec[1]:
             eta = direct_spin1.dev_spin_parity(ci, comb(norb, nelec[0]))
         dev_out = out.reshape(-1) if out is not None and out.is_cuda else None
-        hc = direct_spin1.dev_contract_2e(h2e, ci, norb, nelec, eta=eta, out=dev_out)
+        hc = direct_spin1.dev_contract_2e(h2e, ci, norb, nelec, eta=eta, out=dev_out,
+                                          deterministic=self.deterministic_sigma)
         if h1e_s is not None:
             direct_spin1.dev_contract_1e(h1e_s, -h1e_s, ci, norb, nelec, hc)
         if out is not None:
@@ -514,6 +521,8 @@ class FCISolver(CSFFCISolver, FCIBase):
 
     def _device_resident_ok(self, h1e, eri, norb, nelec, ci0, kwargs):
         if not self.device_resident or ci0 is not None or not set(kwargs) <= self._DEVICE_KW:
+            return False
+        if self.deterministic_sigma:  # the batched plan's sigma uses FP64 atomics
             return False
         if not isinstance(h1e, np.ndarray) or h1e.ndim != 2 or isinstance(eri, torch.Tensor):
             return False

@@ -174,6 +174,57 @@ __global__ void k_sym_add(const double* __restrict__ s, double* out, long long n
   }
 }
 
+// The deterministic mode's sigma from its three int64 digit planes w[k][i]
+// (weights 2^-80, 2^-37, 2^6, see det_add3): out[i] (+)= the value of the
+// digit sums.  Spin-symmetric: out[a][b] (+)= value(S[a][b] + eta S[b][a]),
+// the digits of the two entries added as integers first (exact; the
+// transpose is staged through a shared tile as in k_sym_add).  The three
+// converted terms are exact (|digit sum| < 2^53) and are added in a fixed
+// order, so the result depends on the digit sums alone.
+__device__ __forceinline__ double det_value(long long w0, long long w1, long long w2) {
+  return ((double)w2 * 0x1p6 + (double)w1 * 0x1p-37) + (double)w0 * 0x1p-80;
+}
+
+__global__ void k_det_finish(const long long* __restrict__ w, double* out, long long n, int accumulate) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double v = det_value(w[i], w[n + i], w[2 * n + i]);
+    out[i] = accumulate ? out[i] + v : v;
+  }
+}
+
+__global__ void k_det_finish_sym(const long long* __restrict__ w, double* out, long long na, int eta,
+                                 int accumulate) {
+  __shared__ long long tile[3][32][33];
+  const long long n = na * na;
+  const long long ntile = (na + 31) / 32;
+  for (long long t = blockIdx.x; t < ntile * ntile; t += gridDim.x) {
+    const long long ti = t / ntile, tj = t - ti * ntile;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const long long row = tj * 32 + r, col = ti * 32 + threadIdx.x;
+      const bool in = row < na && col < na;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) tile[k][r][threadIdx.x] = in ? w[k * n + row * na + col] : 0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const long long row = ti * 32 + r, col = tj * 32 + threadIdx.x;
+      if (row < na && col < na) {
+        long long d[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          // two's complement wrap-around: the exact integer sum (mod 2^64)
+          const unsigned long long a = (unsigned long long)w[k * n + row * na + col];
+          const unsigned long long b = (unsigned long long)tile[k][threadIdx.x][r];
+          d[k] = (long long)(eta > 0 ? a + b : a - b);
+        }
+        const double v = det_value(d[0], d[1], d[2]);
+        out[row * na + col] = accumulate ? out[row * na + col] + v : v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // per-block maxima of |c - c^T|, |c + c^T|, |c| over a square n x n matrix
 __global__ void k_parity_part(const double* __restrict__ c, long long n, double* part) {
   __shared__ double s0[256], s1[256], s2[256];
@@ -300,6 +351,8 @@ int csffci_spin_parity(int64_t n, const double* c, double* out3, void* work, siz
 }
 
 size_t csffci_sigma_workspace(int norb, int neleca, int nelecb, int flags) {
+  if (flags & CSFFCI_SIGMA_DETERMINISTIC)  // three int64 digit planes (they hold s in the symmetric mode)
+    return (size_t)(host_binom(norb, neleca) * host_binom(norb, nelecb)) * 3 * sizeof(long long);
   if (flags & CSFFCI_SIGMA_SPIN_SYMMETRIC)
     return (size_t)(host_binom(norb, neleca) * host_binom(norb, nelecb)) * sizeof(double);
   return 0;
@@ -325,6 +378,32 @@ static int sigma_exec(int norb, int neleca, int nelecb, const double* h2e, const
   long long Na = (long long)host_binom(norb, neleca), Nb = (long long)host_binom(norb, nelecb);
   long long ndet = Na * Nb;
   int nla = neleca * (norb - neleca + 1), nlb = nelecb * (norb - nelecb + 1);
+  if (flags & CSFFCI_SIGMA_DETERMINISTIC) {
+    CSF_REQUIRE(!(flags & CSFFCI_SIGMA_REFERENCE_KERNEL),
+                "sigma: the deterministic mode runs the warp-specialised kernel, not the reference kernel");
+    CSF_REQUIRE(norb >= 8 && norb <= 16, "sigma: the deterministic mode covers 8 <= norb <= 16, not %d", norb);
+    const size_t need = csffci_sigma_workspace(norb, neleca, nelecb, flags);
+    if (work == nullptr || work_bytes < need) {
+      set_error("sigma: workspace of %zu bytes < %zu required", work_bytes, need);
+      return CSFFCI_ERR_MEMORY;
+    }
+    if (ndet == 0) return CSFFCI_OK;
+    CSF_CUDA(cudaMemsetAsync(work, 0, need, stream));
+    int st = sigma_rr_run(norb, neleca, nelecb, h2e, link_a, link_b, ci, (double*)work, sym, (double)eta,
+                          stream, -1, ndet);
+    if (st) return st;
+    ProfScope ps("k_det_finish", stream);
+    if (sym) {
+      dim3 blk(32, 8);
+      const long long tiles = ((Na + 31) / 32) * ((Na + 31) / 32);
+      k_det_finish_sym<<<grid_for(tiles, 1, 148 * 16), blk, 0, stream>>>((const long long*)work, sigma, Na, eta,
+                                                                        accumulate ? 1 : 0);
+    } else {
+      k_det_finish<<<grid_for(ndet, 256, 148 * 16), 256, 0, stream>>>((const long long*)work, sigma, ndet,
+                                                                      accumulate ? 1 : 0);
+    }
+    return check_launch("sigma deterministic finish");
+  }
   double* target = sigma;
   if (sym) {
     size_t need = csffci_sigma_workspace(norb, neleca, nelecb, flags);
@@ -435,8 +514,12 @@ int csffci_sigma_plan_create(int norb, int neleca, int nelecb, const double* h2e
               "sigma_plan_create: bad nelec (%d,%d)", neleca, nelecb);
   CSF_REQUIRE(h2e != nullptr && link_a != nullptr && link_b != nullptr,
               "sigma_plan_create: h2e and the link tables are required");
-  CSF_REQUIRE((flags & ~(CSFFCI_SIGMA_SPIN_SYMMETRIC | CSFFCI_SIGMA_REFERENCE_KERNEL)) == 0,
-              "sigma_plan_create: flags may hold SPIN_SYMMETRIC and REFERENCE_KERNEL only");
+  CSF_REQUIRE((flags & ~(CSFFCI_SIGMA_SPIN_SYMMETRIC | CSFFCI_SIGMA_REFERENCE_KERNEL |
+                         CSFFCI_SIGMA_DETERMINISTIC)) == 0,
+              "sigma_plan_create: flags may hold SPIN_SYMMETRIC, REFERENCE_KERNEL and DETERMINISTIC only");
+  CSF_REQUIRE(!(flags & CSFFCI_SIGMA_DETERMINISTIC) ||
+                  (norb >= 8 && norb <= 16 && !(flags & CSFFCI_SIGMA_REFERENCE_KERNEL)),
+              "sigma_plan_create: the deterministic mode covers 8 <= norb <= 16 (warp-specialised kernel)");
   CSF_REQUIRE(!(flags & CSFFCI_SIGMA_SPIN_SYMMETRIC) || neleca == nelecb,
               "sigma_plan_create: the spin-symmetric mode needs neleca == nelecb");
   csffci_sigma_plan_t* p = new (std::nothrow) csffci_sigma_plan_t;
@@ -455,6 +538,7 @@ int csffci_sigma_plan_create(int norb, int neleca, int nelecb, const double* h2e
                    ? -2
                    : sigma_rr_single_variant(norb);
   if (p->variant < 0 && p->variant != -2) p->variant = rr_default_variant(norb);
+  if (flags & CSFFCI_SIGMA_DETERMINISTIC) p->variant = 4;  // the warp-specialised kernel
   p->work_bytes = csffci_sigma_workspace(norb, neleca, nelecb, flags);
   p->work = nullptr;
   if (work_bytes) *work_bytes = p->work_bytes;
@@ -481,7 +565,8 @@ int csffci_sigma_plan_execute(const csffci_sigma_plan_t* plan, const double* ci,
               "sigma_plan_execute: the plan was created without the spin-symmetric mode");
   CSF_REQUIRE(!plan->work_bytes || plan->work != nullptr, "sigma_plan_execute: the plan has no workspace bound");
   return sigma_exec(plan->norb, plan->neleca, plan->nelecb, plan->h2e, plan->link_a, plan->link_b, ci, sigma,
-                    flags | (plan->flags & CSFFCI_SIGMA_REFERENCE_KERNEL), eta, plan->work, plan->work_bytes,
+                    flags | (plan->flags & (CSFFCI_SIGMA_REFERENCE_KERNEL | CSFFCI_SIGMA_DETERMINISTIC)), eta,
+                    plan->work, plan->work_bytes,
                     plan->variant, stream);
 }
 

@@ -122,9 +122,12 @@ static void rr_prepare(int norb, int njobs, csffci_sigma_job_t* jobs, long long*
 
 int sigma_rr_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev,
                     const csffci_sigma_job_t& job0, long long total_units, long long max_nb,
-                    int max_nla, int max_nlb, cudaStream_t stream, int variant) {
+                    int max_nla, int max_nlb, cudaStream_t stream, int variant, long long det_stride) {
   const int npair = norb * (norb + 1) / 2;
   const int ks = (npair + 3) / 4;
+  if (det_stride)  // the deterministic scatter exists in the warp-specialised kernel only
+    return sigma_ws_launch(norb, njobs, jobs_dev, job0, total_units, max_nb, max_nla, max_nlb, stream, 8,
+                           det_stride);
   if (variant < 0 && !jobs_dev) variant = sigma_rr_single_variant(norb);
   if (variant < 0) variant = rr_default_variant(norb);
   if (variant == RR_VARIANT_WS || variant == RR_VARIANT_WS16)
@@ -146,6 +149,7 @@ int sigma_rr_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev,
   const int nt = kVariantShape[variant][1];
   const int nb = 8 * nt;
   RRArgs g;
+  memset(&g, 0, sizeof(g));
   g.jobs = jobs_dev;
   g.job0 = job0;
   g.njobs = njobs;
@@ -183,7 +187,7 @@ switch (variant) {
 
 int sigma_rr_run(int norb, int neleca, int nelecb, const double* h2e, const csffci_link_t* la,
                  const csffci_link_t* lb, const double* ci, double* out, bool sym, double eta,
-                 cudaStream_t stream, int variant) {
+                 cudaStream_t stream, int variant, long long det_stride) {
   CSF_REQUIRE(rr_aligned8(la) && rr_aligned8(lb) && rr_aligned8(ci) && rr_aligned8(out),
               "sigma: link tables and vectors must be 8-byte aligned");
   csffci_sigma_job_t J;
@@ -201,7 +205,7 @@ int sigma_rr_run(int norb, int neleca, int nelecb, const double* h2e, const csff
   long long total, maxnb;
   int mla, mlb;
   rr_prepare(norb, 1, &J, &total, &maxnb, &mla, &mlb);
-  return sigma_rr_launch(norb, 1, nullptr, J, total, maxnb, mla, mlb, stream, variant);
+  return sigma_rr_launch(norb, 1, nullptr, J, total, maxnb, mla, mlb, stream, variant, det_stride);
 }
 
 // ---- batch: zero the outputs, run the jobs, form sigma = S + eta S^T -----

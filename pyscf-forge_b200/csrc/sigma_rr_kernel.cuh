@@ -35,7 +35,35 @@ struct RRArgs {
   int bulk;            // warp-specialised kernels: alpha rows by bulk copy
   int parts;           // warp-specialised kernels: parts of each row unit from split_from on
   long long split_from;  // warp-specialised kernels: first row unit cut into parts
+  long long det_stride;  // deterministic mode: elements between the digit planes (0: FP64 atomics)
 };
+
+// Deterministic scatter: x = d2 2^6 + d1 2^-37 + d0 2^-80 with integer
+// digits |d_k| <= 2^42 (for |x| < 2^48; larger x up to 2^55 only widens
+// d2), each added to its own int64 plane by an integer atomic.  Integer
+// addition is associative, so the plane sums do not depend on the order of
+// the contributions.  Every step is exact except the rounding of d0 (below
+// 2^-80), which depends on x alone: x - 64 h2 and r1 - 2^-37 h1 are exactly
+// representable (the remainder keeps the low bits of x), so fma returns
+// them without rounding.
+__device__ __forceinline__ void det_add3(double* p, long long stride, double x) {
+  const double h2 = rint(x * 0x1p-6);
+  const double r1 = fma(-h2, 0x1p6, x);
+  const double h1 = rint(r1 * 0x1p37);
+  const double r0 = fma(-h1, 0x1p-37, r1);
+  const double h0 = rint(r0 * 0x1p80);
+  unsigned long long* w = reinterpret_cast<unsigned long long*>(p);
+  atomicAdd(w, (unsigned long long)(long long)h0);
+  atomicAdd(w + stride, (unsigned long long)(long long)h1);
+  atomicAdd(w + 2 * stride, (unsigned long long)(long long)h2);
+}
+
+// one scattered contribution: an FP64 atomic, or the three digit atomics
+template <bool DET>
+__device__ __forceinline__ void ws_out_add(double* p, double x, long long stride) {
+  if (DET) det_add3(p, stride, x);
+  else atomicAdd(p, x);
+}
 
 // Alpha link of the current row Ja as the tile loops use it: the offset
 // Ka*Nb of its row of c (copies) and of sigma (alpha scatter), the offset
@@ -428,7 +456,7 @@ bool sigma_ws_supported(int norb);
 bool sigma_ws16_supported(int norb);
 int sigma_ws_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev, const csffci_sigma_job_t& job0,
                     long long total_units, long long max_nb, int max_nla, int max_nlb, cudaStream_t stream,
-                    int mw);
+                    int mw, long long det_stride = 0);
 // the warp-specialised kernel with registers re-split between the roles
 // (sigma_wsr.cu), one problem at 16 orbitals
 constexpr int RR_VARIANT_WSR = 5;
@@ -443,7 +471,7 @@ bool batch_variant_valid(int norb, int v);
 int rr_default_variant(int norb);
 int sigma_rr_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev, const csffci_sigma_job_t& job0,
                     long long total_units, long long max_nb, int max_nla, int max_nlb, cudaStream_t stream,
-                    int variant);
+                    int variant, long long det_stride = 0);
 int rr_dispatch_v0(int norb, RRArgs& g, size_t smem, cudaStream_t stream);  // (16, 4)
 int rr_dispatch_v1(int norb, RRArgs& g, size_t smem, cudaStream_t stream);  // (8, 4)
 int rr_dispatch_v2(int norb, RRArgs& g, size_t smem, cudaStream_t stream);  // (16, 2)

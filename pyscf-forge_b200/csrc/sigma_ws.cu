@@ -55,7 +55,7 @@ struct WSLayout {
 
 constexpr int WS_RU = 4;      // links a mover thread handles together (loads in flight)
 
-template <int KS, int MT, int MW, bool BATCH, int MINB>
+template <int KS, int MT, int MW, bool BATCH, int MINB, bool DET = false>
 __global__ void __launch_bounds__(WSLayout<MT, MW>::NTOT * 32, MINB) k_sigma_ws(RRArgs g) {
   using L = WSLayout<MT, MW>;
   constexpr int NB = WS_NB;
@@ -188,8 +188,9 @@ __global__ void __launch_bounds__(WSLayout<MT, MW>::NTOT * 32, MINB) k_sigma_ws(
                 const unsigned aneg = S.pneg[srow.pc + r];
 #pragma unroll
                 for (int t = 0; t < 2; ++t) {
-                  if (J + 8 * t < alim) atomicAdd(abase + J + 8 * t, rr_flip(acc[t][2 * h], aneg));
-                  if (J + 8 * t + 1 < alim) atomicAdd(abase + J + 8 * t + 1, rr_flip(acc[t][2 * h + 1], aneg));
+                  if (J + 8 * t < alim) ws_out_add<DET>(abase + J + 8 * t, rr_flip(acc[t][2 * h], aneg), g.det_stride);
+                  if (J + 8 * t + 1 < alim)
+                    ws_out_add<DET>(abase + J + 8 * t + 1, rr_flip(acc[t][2 * h + 1], aneg), g.det_stride);
                 }
               }
             }
@@ -231,18 +232,18 @@ __global__ void __launch_bounds__(WSLayout<MT, MW>::NTOT * 32, MINB) k_sigma_ws(
             const unsigned aneg = S.pneg[srow.pc + r0];
             const int alim = (int)(sjob.sym ? srow.ja : sjob.Nb);
             const int J = (srow.c0 + c) * NB + 8 * t0 + 2 * tq;
-            if (J < alim) atomicAdd(abase + J, rr_flip(acc[0][0], aneg));
-            if (J + 1 < alim) atomicAdd(abase + J + 1, rr_flip(acc[0][1], aneg));
+            if (J < alim) ws_out_add<DET>(abase + J, rr_flip(acc[0][0], aneg), g.det_stride);
+            if (J + 1 < alim) ws_out_add<DET>(abase + J + 1, rr_flip(acc[0][1], aneg), g.det_stride);
             if (!part) {
-              if (J + 8 < alim) atomicAdd(abase + J + 8, rr_flip(acc[1][0], aneg));
-              if (J + 9 < alim) atomicAdd(abase + J + 9, rr_flip(acc[1][1], aneg));
+              if (J + 8 < alim) ws_out_add<DET>(abase + J + 8, rr_flip(acc[1][0], aneg), g.det_stride);
+              if (J + 9 < alim) ws_out_add<DET>(abase + J + 9, rr_flip(acc[1][1], aneg), g.det_stride);
             }
           }
         }
       }
     }
   } else {
-    ws_mover_role<NTH, NMOV, WS_RU, BATCH>(g, S, tid, warp, lane, tid - NWM * 32, warp - NWM);
+    ws_mover_role<NTH, NMOV, WS_RU, BATCH, DET>(g, S, tid, warp, lane, tid - NWM * 32, warp - NWM);
   }
 }
 
@@ -257,9 +258,12 @@ constexpr int ws_min_blocks(int norb) { return norb <= 12 ? 2 : 1; }
 template <int KS, int MT, int NORB, int MW>
 static int launch_ws(RRArgs& g, size_t smem, cudaStream_t stream) {
   constexpr int NTH = WSLayout<MT, MW>::NTOT * 32;
-  // 16-row MMA warps: 8-warp CTAs, three per SM
+  // 16-row MMA warps: 8-warp CTAs, two per SM
   constexpr int MINB = MW == 16 ? 2 : ws_min_blocks(NORB);
-  auto kern = g.jobs ? k_sigma_ws<KS, MT, MW, true, MINB> : k_sigma_ws<KS, MT, MW, false, MINB>;
+  // the deterministic scatter: one problem, 8-row MMA warps only
+  auto kern = g.jobs ? k_sigma_ws<KS, MT, MW, true, MINB>
+              : (MW == 8 && g.det_stride) ? k_sigma_ws<KS, MT, MW, false, MINB, MW == 8>
+                                          : k_sigma_ws<KS, MT, MW, false, MINB>;
   CSF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, nsm = 148, per_sm = 0;
   CSF_CUDA(cudaGetDevice(&dev));
@@ -279,7 +283,7 @@ static int launch_ws(RRArgs& g, size_t smem, cudaStream_t stream) {
   static const char* names16[13] = {"", "", "", "", "", "", "", "", "k_sigma_ws16_n8", "k_sigma_ws16_n9",
                                     "k_sigma_ws16_n10", "k_sigma_ws16_n11", "k_sigma_ws16_n12"};
   const char* name = MW == 16 ? (g.jobs ? names16[NORB <= 12 ? NORB : 0] : "k_sigma_ws16")
-                              : (g.jobs ? names8[NORB] : "k_sigma_ws");
+                              : (g.jobs ? names8[NORB] : g.det_stride ? "k_sigma_ws_det" : "k_sigma_ws");
   ProfScope ps(name, stream);
   kern<<<(int)grid, NTH, smem, stream>>>(g);
   return check_launch("sigma (warp-specialised)");
@@ -317,9 +321,13 @@ size_t ws_layout(RRArgs& g, int npair, int rows_multiple, long long max_nb, int 
 
 int sigma_ws_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev, const csffci_sigma_job_t& job0,
                     long long total_units, long long max_nb, int max_nla, int max_nlb, cudaStream_t stream,
-                    int mw) {
+                    int mw, long long det_stride) {
   if (!(mw == 8 ? sigma_ws_supported(norb) : sigma_ws16_supported(norb))) {
     set_error("sigma: no warp-specialised kernel with %d-row MMA warps for norb %d", mw, norb);
+    return CSFFCI_ERR_INVALID;
+  }
+  if (det_stride && (jobs_dev || mw != 8)) {
+    set_error("sigma: the deterministic scatter takes one problem and 8-row MMA warps");
     return CSFFCI_ERR_INVALID;
   }
   const int npair = norb * (norb + 1) / 2;
@@ -331,6 +339,7 @@ int sigma_ws_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev, con
   g.parts = 1;
   g.split_from = total_units;
   g.total_units = total_units;
+  g.det_stride = det_stride;
   const size_t smem = ws_layout(g, npair, mw, max_nb, max_nla, max_nlb, 0, nullptr);
   if (smem == 0) {
     set_error("sigma: warp-specialised tiles exceed shared memory (norb %d)", norb);

@@ -211,7 +211,7 @@ __device__ __forceinline__ bool ws_row_setup(const RRArgs& g, const WSShared& S,
 // together, every load of the pass issued before the dependent ones (a
 // mover is often the only warp of the role on its scheduler, so this
 // instruction-level parallelism is its way to hide latency).
-template <int NTH, int NMOV, int RU, bool BATCH>
+template <int NTH, int NMOV, int RU, bool BATCH, bool DET = false>
 __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S, int tid, int warp, int lane,
                                               int mtid, int mwarp) {
   constexpr int NB = WS_NB;
@@ -357,7 +357,7 @@ __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S
               for (int k = 0; k < RU; ++k) v[k] = D[rr_lpair(e[k]) * ds + jl];
 #pragma unroll
               for (int k = 0; k < RU; ++k)
-                if (m0 + k * MPASS < nlb) atomicAdd(&orow[e[k].x], rr_flip(v[k], rr_lneg(e[k])));
+                if (m0 + k * MPASS < nlb) ws_out_add<DET>(&orow[e[k].x], rr_flip(v[k], rr_lneg(e[k])), g.det_stride);
             }
           }
         }

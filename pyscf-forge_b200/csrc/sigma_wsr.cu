@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(WSR_NTH, 1) k_sigma_wsr(RRArgs g) {
   } else {
     wsr_reg_dec<WSR_REG_MOV>();
     const int mw = warp - WSR_NBIG - WSR_NTAIL;
-    ws_mover_role<WSR_NTH, WSR_NMOV, WSR_RU, false>(g, S, tid, warp, lane, mw * 32 + lane, mw);
+    ws_mover_role<WSR_NTH, WSR_NMOV, WSR_RU, false, false>(g, S, tid, warp, lane, mw * 32 + lane, mw);
   }
 }
 

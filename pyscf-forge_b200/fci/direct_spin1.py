@@ -95,9 +95,10 @@ class SigmaPlan:
     the reference's fci_contract_gas_plan, pyscf/lib/mcscf/fci_gas.h:244-253).
     Holds references to h2e and the link tables, whose device memory the
     plan borrows; the kernel is fixed at creation (CSFFCI_SIGMA_VARIANT is
-    read then)."""
+    read then).  deterministic: the scatter of CSFFCI_SIGMA_DETERMINISTIC
+    (bit-identical reruns, 8 <= norb <= 16)."""
 
-    def __init__(self, h2e, norb, nelec, spin_symmetric=False):
+    def __init__(self, h2e, norb, nelec, spin_symmetric=False, deterministic=False):
         require_cuda()
         na, nb = nelec
         self.norb, self.nelec = int(norb), (int(na), int(nb))
@@ -105,7 +106,10 @@ class SigmaPlan:
         self.la = dev_link_table(norb, na)
         self.lb = dev_link_table(norb, nb)
         self.sym = bool(spin_symmetric) and na == nb
+        self.deterministic = bool(deterministic)
         flags = _capi.SIGMA_SPIN_SYMMETRIC if self.sym else 0
+        if self.deterministic:
+            flags |= _capi.SIGMA_DETERMINISTIC
         h = ctypes.c_void_p()
         nbytes = ctypes.c_size_t()
         _capi.call("csffci_sigma_plan_create", self.norb, na, nb, ptr(self.h2e), ptr(self.la), ptr(self.lb),
@@ -134,33 +138,37 @@ class SigmaPlan:
 
     def __del__(self):
         h, self._h = getattr(self, "_h", None), None
-        if h is not None and _capi._LIB is not None:
-            _capi._LIB.csffci_sigma_plan_destroy(h)
+        # at interpreter exit the module globals may already be gone
+        lib = getattr(_capi, "_LIB", None) if _capi is not None else None
+        if h is not None and lib is not None:
+            lib.csffci_sigma_plan_destroy(h)
 
 
 _PLAN_CACHE = {}
 _PLAN_CACHE_SIZE = 8
 
 
-def sigma_plan(h2e, norb, nelec):
-    """The cached SigmaPlan of (device, norb, nelec, h2e tensor); the cache
-    keeps the h2e tensor alive, so its address names it, and holds at most
-    _PLAN_CACHE_SIZE plans (least recently used dropped first)."""
+def sigma_plan(h2e, norb, nelec, deterministic=False):
+    """The cached SigmaPlan of (device, norb, nelec, h2e tensor, scatter
+    mode); the cache keeps the h2e tensor alive, so its address names it,
+    and holds at most _PLAN_CACHE_SIZE plans (least recently used dropped
+    first)."""
     key = (torch.cuda.current_device(), int(norb), int(nelec[0]), int(nelec[1]), h2e.data_ptr(),
-           tuple(h2e.shape))
+           tuple(h2e.shape), bool(deterministic))
     plan = _PLAN_CACHE.pop(key, None)
     if plan is None or plan.h2e.data_ptr() != h2e.data_ptr():
-        plan = SigmaPlan(h2e, norb, nelec, spin_symmetric=nelec[0] == nelec[1])
+        plan = SigmaPlan(h2e, norb, nelec, spin_symmetric=nelec[0] == nelec[1], deterministic=deterministic)
     _PLAN_CACHE[key] = plan
     while len(_PLAN_CACHE) > _PLAN_CACHE_SIZE:
         _PLAN_CACHE.pop(next(iter(_PLAN_CACHE)))
     return plan
 
 
-def dev_contract_2e(h2e, ci, norb, nelec, eta=None, out=None, accumulate=False):
+def dev_contract_2e(h2e, ci, norb, nelec, eta=None, out=None, accumulate=False, deterministic=False):
     """sigma = sum h2e[pq,rs] E_pq E_rs ci on the device.  eta (+1/-1) asserts
-    ci = eta ci^T (na == nb) and selects the row-local kernel.  Runs through
-    the cached sigma plan of (norb, nelec, h2e)."""
+    ci = eta ci^T (na == nb) and selects the row-local kernel; deterministic
+    selects the order-independent scatter (bit-identical reruns).  Runs
+    through the cached sigma plan of (norb, nelec, h2e, scatter mode)."""
     na, nb = nelec
     ci = ci.contiguous()
     if out is None:
@@ -175,12 +183,14 @@ def dev_contract_2e(h2e, ci, norb, nelec, eta=None, out=None, accumulate=False):
         flags = _capi.SIGMA_ACCUMULATE if accumulate else 0
         if eta is not None:
             flags |= _capi.SIGMA_SPIN_SYMMETRIC
+        if deterministic:
+            flags |= _capi.SIGMA_DETERMINISTIC
         nbytes = _capi.query("csffci_sigma_workspace", norb, na, nb, flags)
         ws = workspace("sigma", nbytes) if nbytes else None
         _capi.call("csffci_sigma", norb, na, nb, ptr(h2e), ptr(la), ptr(lb), ptr(ci), ptr(out), flags,
                    int(eta or 1), ptr(ws), nbytes, stream())
         return out
-    return sigma_plan(h2e, norb, (na, nb))(ci, out, eta=eta, accumulate=accumulate)
+    return sigma_plan(h2e, norb, (na, nb), deterministic)(ci, out, eta=eta, accumulate=accumulate)
 
 
 def dev_spin_parity(ci, n, rtol=1e-12):
