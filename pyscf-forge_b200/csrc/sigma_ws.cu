@@ -1,5 +1,10 @@
-// Warp-specialised variant of the register-resident sigma kernel (tile
-// variant 4), for one problem at 13..16 orbitals.
+// Warp-specialised variant of the register-resident sigma kernel, 8..16
+// orbitals: tile variant 4 (one MMA warp per 8 rows) and, up to 12 orbitals,
+// variant 7 (one MMA warp per 16 rows, m16n8k4, in CTAs of 8 warps).  Either
+// runs one problem or a job table of many (BATCH: each unit's job is looked
+// up between two barrier-9 syncs, gated jobs are skipped by both roles); the
+// one-problem form with 8-row warps also has the deterministic scatter (DET:
+// integer digit planes instead of FP64 atomics, det_add3).
 //
 // k_sigma_rr runs the gather, MMA and scatter phases of a tile one after the
 // other, separated by block barriers, so the FP64 tensor pipe idles while
@@ -29,6 +34,7 @@
 // The CTA has a multiple of four warps, so every scheduler gets the same
 // number; at 16 orbitals that is 17 MMA warps and 3 movers, 5 warps per
 // scheduler: the register budget of k_sigma_rr, which the A fragments need.
+// Up to 12 orbitals the fragments are small enough for two CTAs per SM.
 #include <stdlib.h>
 
 #include "sigma_ws.cuh"
