@@ -804,40 +804,30 @@ int enqueue_iteration_km(csffci_batch_plan_t* P, cudaStream_t s) {
 #define DB_CHECK(what)                 \
   if ((st = check_launch(what)) != 0) \
     return st;
-  {
-    ProfScope ps("k_db_proj", s);
-    k_db_proj<KM, 0><<<gs, DB_NT, P->smem_stream, s>>>(a);
-    DB_CHECK("batch solver: projection 0");
-    k_db_sproj<0><<<np, DB_ST, 0, s>>>(a);
-    DB_CHECK("batch solver: projection 0 reduce");
-    k_db_proj<KM, 1><<<gs, DB_NT, P->smem_stream, s>>>(a);
-    DB_CHECK("batch solver: projection 1");
-    k_db_sproj<1><<<np, DB_ST, 0, s>>>(a);
-    DB_CHECK("batch solver: projection 1 reduce");
-    k_db_proj<KM, 2><<<gs, DB_NT, P->smem_stream, s>>>(a);
-    DB_CHECK("batch solver: projection 2");
-    k_db_sproj<2><<<np, DB_ST, 0, s>>>(a);
-    DB_CHECK("batch solver: orthonormalisation");
-    k_db_new<KM><<<gs, DB_NT, 0, s>>>(a);
-    DB_CHECK("batch solver: new vectors");
-  }
+  // one profiler scope per launch (timed only while profiling is enabled)
+#define DB_LAUNCH(name, what, ...)  \
+  {                                 \
+    ProfScope ps_(name, s);         \
+    __VA_ARGS__;                    \
+  }                                 \
+  DB_CHECK(what)
+  DB_LAUNCH("k_db_proj", "batch solver: projection 0", (k_db_proj<KM, 0><<<gs, DB_NT, P->smem_stream, s>>>(a)));
+  DB_LAUNCH("k_db_sproj", "batch solver: projection 0 reduce", (k_db_sproj<0><<<np, DB_ST, 0, s>>>(a)));
+  DB_LAUNCH("k_db_proj", "batch solver: projection 1", (k_db_proj<KM, 1><<<gs, DB_NT, P->smem_stream, s>>>(a)));
+  DB_LAUNCH("k_db_sproj", "batch solver: projection 1 reduce", (k_db_sproj<1><<<np, DB_ST, 0, s>>>(a)));
+  DB_LAUNCH("k_db_proj", "batch solver: projection 2", (k_db_proj<KM, 2><<<gs, DB_NT, P->smem_stream, s>>>(a)));
+  DB_LAUNCH("k_db_sproj", "batch solver: orthonormalisation", (k_db_sproj<2><<<np, DB_ST, 0, s>>>(a)));
+  DB_LAUNCH("k_db_new", "batch solver: new vectors", (k_db_new<KM><<<gs, DB_NT, 0, s>>>(a)));
   if ((st = transform_batch_launch(1, P->drev, (int)P->jrev.size(), P->trev, s)) != 0) return st;
   for (size_t g = 0; g < P->group_info.size(); ++g)
     if ((st = sigma_batch_launch(P->group_info[g], P->group_dev[g], s)) != 0) return st;
   if ((st = transform_batch_launch(0, P->dfwd, (int)P->jfwd.size(), P->tfwd, s)) != 0) return st;
-  {
-    ProfScope ps("k_db_ritz", s);
-    k_db_hv<KM><<<gs, DB_NT, P->smem_stream, s>>>(a);
-    DB_CHECK("batch solver: H v");
-    k_db_sritz<<<np, DB_ST, P->smem_ritz, s>>>(a);
-    DB_CHECK("batch solver: subspace eigenproblem");
-    k_db_ritz<KM><<<gs, DB_NT, P->smem_stream, s>>>(a);
-    DB_CHECK("batch solver: Ritz vectors");
-    k_db_sconv<<<np, DB_ST, 0, s>>>(a);
-    DB_CHECK("batch solver: convergence");
-    k_db_pre<<<gs, DB_NT, 0, s>>>(a);
-    DB_CHECK("batch solver: preconditioner");
-  }
+  DB_LAUNCH("k_db_hv", "batch solver: H v", (k_db_hv<KM><<<gs, DB_NT, P->smem_stream, s>>>(a)));
+  DB_LAUNCH("k_db_sritz", "batch solver: subspace eigenproblem", (k_db_sritz<<<np, DB_ST, P->smem_ritz, s>>>(a)));
+  DB_LAUNCH("k_db_ritz", "batch solver: Ritz vectors", (k_db_ritz<KM><<<gs, DB_NT, P->smem_stream, s>>>(a)));
+  DB_LAUNCH("k_db_sconv", "batch solver: convergence", (k_db_sconv<<<np, DB_ST, 0, s>>>(a)));
+  DB_LAUNCH("k_db_pre", "batch solver: preconditioner", (k_db_pre<<<gs, DB_NT, 0, s>>>(a)));
+#undef DB_LAUNCH
 #undef DB_CHECK
   return CSFFCI_OK;
 }
