@@ -360,6 +360,7 @@ def run_ours(args, rank_env):
         line["rdm"] = run_rdm(dmma)
     if rank == 0 and world == 1 and not args.no_batched:
         line["batched"] = run_batched(args.batch)
+        line["batched"]["transforms"] = run_batch_transforms()
     if rank == 0 and world == 1 and not args.no_c4:
         line["c4"] = run_c4(ref_check=not args.no_cpu_baseline)
     if rank == 0 and world == 1 and not args.no_rdm:
@@ -535,6 +536,45 @@ def run_c4(ref_check=True):
             "rayleigh_quotient_minus_e0": e0 - float(E[0].detach()),
             "residual_norm": float(np.linalg.norm(hc0 - float(E[0].detach()) * c0)),
             "note": "the reference's CPU sigma (libfci_gas, one GAS subspace) applied to root 0"}
+    return out
+
+
+def run_batch_transforms(reps=3):
+    """The batched det<->CSF transforms (csffci_transform_batch, one launch
+    over every problem) on the CSF spaces of the 128-problem batch, one
+    vector per root, device-timed per launch (k_transform_batch), with the
+    fraction of the HBM roofline on the compulsory bytes 8*(ndet+ncsf) +
+    4*ndet per vector."""
+    import numpy as np
+    import torch
+    from pyscf_forge_b200 import _capi
+    from pyscf_forge_b200 import batched as Bt
+    from pyscf_forge_b200.csf_fci.csfstring import CSFTransformer
+    hbm, src = peaks()
+    g = torch.Generator(device="cpu").manual_seed(11)
+    items, nbytes = [], 0
+    for p in Bt.make_uneven_batch(128):
+        t = CSFTransformer(p.norb, p.nelec[0], p.nelec[1], p.smult)
+        x = torch.randn(p.nroots, t.ncsf, generator=g, dtype=torch.float64).cuda()
+        items.append((t, x))
+        nbytes += p.nroots * (8 * (t.ndet + t.ncsf) + 4 * t.ndet)
+    dets = Bt.transform_many(items, reverse=True)
+    back = [(t, d) for (t, _), d in zip(items, dets)]
+    out = {"workload": "C3 batch spaces, one vector per root (%d vectors)" % sum(x.shape[0] for _, x in items),
+           "algorithmic_bytes": nbytes}
+    for name, its, rev in (("csf2det", items, True), ("det2csf", back, False)):
+        Bt.transform_many(its, reverse=rev)
+        _capi.profile_enable(True)
+        for _ in range(reps):
+            Bt.transform_many(its, reverse=rev)
+        prof = _capi.profile_report()
+        _capi.profile_enable(False)
+        n, tot = prof.get("k_transform_batch", (0, 0.0))
+        ms = tot / max(n, 1)
+        out[name] = {"kernel_ms": round(ms, 4), "GBps": nbytes / ms / 1e6, "frac_hbm": nbytes / ms / 1e6 / hbm}
+    err = max(float((y - x).abs().max()) for (_, x), y in zip(items, Bt.transform_many(back, reverse=False)))
+    out["round_trip_max_abs_err"] = err
+    out["peak_note"] = "hbm_gbs %s" % src
     return out
 
 
