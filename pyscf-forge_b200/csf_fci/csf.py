@@ -127,9 +127,15 @@ def pspace(fci, h1e, eri, norb, nelec, transformer, hdiag_det=None, hdiag_csf=No
            max_memory=None):
     """csf.py:246-366: the lowest-diagonal CSFs, completed to whole
     configurations, with H built over their determinants by Slater-Condon
-    rules and transformed to the CSF basis."""
+    rules and transformed to the CSF basis.  max_memory (MB; default
+    fci.max_memory) bounds the p-space matrices as at csf.py:294-303:
+    MemoryError when 1.2 * 8 * (npsp_det + npsp_csf)^2 bytes exceed it (here
+    the matrices live in device memory, so the budget is the device buffer's,
+    not the host process's growth)."""
     if norb > 63:
         raise NotImplementedError('norb > 63')
+    if max_memory is None:
+        max_memory = getattr(fci, 'max_memory', None)
     neleca, nelecb = _unpack_nelec(nelec)
     eri4 = to_dev(eri_pair_matrix(eri, norb))
     if hdiag_det is None:
@@ -154,6 +160,10 @@ def pspace(fci, h1e, eri, norb, nelec, transformer, hdiag_det=None, hdiag_csf=No
     econf = torch.unique(transformer.econf_csf_mask[csf_addr].long()).cpu().numpy()
     det_addr = _conf_dets(transformer, econf)
     n = det_addr.numel()
+    mem_h0 = 1.2 * (n + npsp_csf) ** 2.0 * 8 / 1e6
+    if max_memory is not None and mem_h0 > max_memory:
+        raise MemoryError("pspace_size of {} CSFs -> {} determinants requires {} MB, cf {} MB "
+                          "remaining memory".format(npsp_csf, n, mem_h0, max_memory))
     ha, hb = unpack_h1e_ab(h1e)
     h1a, h1b = to_dev(ha), to_dev(hb)
     h0 = torch.empty((n, n), dtype=torch.float64, device=device())
@@ -483,7 +493,7 @@ class CSFFCISolver:
             self.smult = kwargs.pop('smult')
         self.check_transformer_cache()
         return pspace(self, h1e, eri, norb, nelec, self.transformer, hdiag_det=hdiag_det,
-                      hdiag_csf=hdiag_csf, npsp=npsp)
+                      hdiag_csf=hdiag_csf, npsp=npsp, max_memory=kwargs.get('max_memory', self.max_memory))
 
     def log_transformer_cache(self, tverbose=0, **kwargs):
         if len(kwargs):

@@ -369,6 +369,18 @@ def test_errors_are_raised():
     t = C.CSFTransformer(6, 3, 3, 1)
     with pytest.raises(C.ImpossibleCIvecError):
         t.vec_det2csf(np.zeros(17))
+    # the p-space memory guard of csf.py:294-303, driven by a memory budget
+    # (max_memory in MB): here 20 CSFs need about 0.07 MB
+    from conftest import seeded_integrals
+    h1, eri = seeded_integrals(6, 12, seed=2)
+    sol = P.csf_solver(None, smult=1)
+    with pytest.raises(MemoryError):
+        sol.pspace(h1, eri, 6, (3, 3), npsp=20, max_memory=0.01)
+    sol.pspace(h1, eri, 6, (3, 3), npsp=20, max_memory=1.0)
+    sol.max_memory = 0.01
+    sol.device_resident = False
+    with pytest.raises(MemoryError):
+        sol.kernel(h1, eri, 6, (3, 3))
 
 
 @pytest.mark.parametrize("norb,nelec,smult", [(8, (4, 4), 1), (10, (5, 5), 3), (12, (6, 6), 1),
