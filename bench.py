@@ -361,6 +361,7 @@ def run_ours(args, rank_env):
     if rank == 0 and world == 1 and not args.no_batched:
         line["batched"] = run_batched(args.batch)
         line["batched"]["transforms"] = run_batch_transforms()
+        line["solves"] = run_solves()
     if rank == 0 and world == 1 and not args.no_c4:
         line["c4"] = run_c4(ref_check=not args.no_cpu_baseline)
     if rank == 0 and world == 1 and not args.no_rdm:
@@ -536,6 +537,59 @@ def run_c4(ref_check=True):
             "rayleigh_quotient_minus_e0": e0 - float(E[0].detach()),
             "residual_norm": float(np.linalg.norm(hc0 - float(E[0].detach()) * c0)),
             "note": "the reference's CPU sigma (libfci_gas, one GAS subspace) applied to root 0"}
+    return out
+
+
+SOLVE_CONFIGS = {"C0": (8, (4, 4), 1, 1, 16), "C1": (12, (6, 6), 1, 3, 24), "C2": (14, (7, 7), 3, 2, 28)}
+
+
+def run_solves():
+    """The single-problem configurations C0 (norb 8 (4,4) singlet, 1 root),
+    C1 (norb 12 (6,6) singlet, 3 roots) and C2 (norb 14 (7,7) triplet, 2
+    roots), seeded integrals of rank 16/24/28: a fresh FCISolver.kernel plus
+    make_rdm12 of every root, end to end (host integrals in, host energies,
+    CI vectors and RDMs out), timed on the second of two runs.  Settings are
+    those of the reference timing (conv_tol 1e-10, max_cycle 400,
+    max_space 30).  Beside each: the reference's own csf.py kernel +
+    make_rdm12 on the same problem (tests/golden/ref_solves_c0_c2.jsonl,
+    made by oracle/time_reference_solves.py in the build container on 8
+    threads: a reported baseline from another host) and the energy
+    difference from it."""
+    import numpy as np
+    import torch
+    import pyscf_forge_b200 as P
+    ref = {}
+    path = os.path.join(ROOT, "tests", "golden", "ref_solves_c0_c2.jsonl")
+    if os.path.exists(path):
+        for l in open(path):
+            d = json.loads(l)
+            ref[d["config"]] = d
+    out = {}
+    for tag, (norb, nelec, smult, nroots, rank) in SOLVE_CONFIGS.items():
+        h1, eri = seeded_integrals(norb, rank)
+        for _ in range(2):
+            sol = P.csf_solver(None, smult=smult)
+            sol.nroots, sol.conv_tol, sol.max_cycle, sol.max_space = nroots, 1e-10, 400, 30
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            e, ci = sol.kernel(h1, eri, norb, nelec)
+            cis = ci if isinstance(ci, list) else [ci]
+            rdms = [sol.make_rdm12(c, norb, nelec) for c in cis]
+            torch.cuda.synchronize()
+            t = time.perf_counter() - t0
+        e = np.atleast_1d(np.asarray(e, dtype=float))
+        row = {"seconds": t, "solves_rdms_per_s": 1.0 / t, "energies": [float(x) for x in e],
+               "converged": [bool(x) for x in np.atleast_1d(sol.converged)],
+               "trace_dm1_minus_n": max(abs(float(np.trace(r[0])) - sum(nelec)) for r in rdms)}
+        if tag in ref:
+            r = ref[tag]
+            row["max_abs_dE_vs_reference"] = float(np.max(np.abs(e - np.asarray(r["energies"]))))
+            rs = r["solve_s"] + r["rdm_s"]
+            row["reference_cpu"] = {"seconds": rs, "threads": r["threads"],
+                                    "note": "reference csf.py kernel + make_rdm12 on the stand-in, build "
+                                            "container, not this host"}
+            row["speedup_vs_reference_cpu"] = rs / t
+        out[tag] = row
     return out
 
 

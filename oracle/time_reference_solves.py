@@ -14,9 +14,12 @@ make_rdm12 of every root, for the single-problem configurations:
 Solver settings: conv_tol 1e-10, max_cycle 400, max_space 30 (the seeded
 integrals are weakly diagonally dominant; see tests/golden/make_c3_golden.py).
 Prints one JSON line per configuration: seconds, solves+RDMs per second,
-energies, threads.
+energies, threads.  Its output of the three configurations (8 threads in
+the build container) is committed as tests/golden/ref_solves_c0_c2.jsonl,
+which bench.py reads for the reference energies and CPU times it reports
+beside the GPU solves:
 
-    python oracle/time_reference_solves.py [C0 C1 C2]
+    python oracle/time_reference_solves.py C0 C1 C2 > tests/golden/ref_solves_c0_c2.jsonl
 """
 import json
 import os
