@@ -21,7 +21,12 @@ at CAS(16,16) (one root) and CAS(14,14) (two roots state-averaged).
 
 ``batched`` (same line, rank 0 at N=1): solves+RDMs/s of 128 seeded uneven
 problems through the device-resident batched solver, next to the plain
-one-problem-at-a-time GPU form on the same problems (run_batched).
+one-problem-at-a-time GPU form on the same problems (run_batched), and the
+batched det<->CSF transform throughput on their spaces.
+
+``solves`` (same line, rank 0 at N=1): the single-problem configurations
+C0-C2 end to end, beside the reference solver's timings and energies
+(run_solves).
 
 Reference arm: the reference's own CPU sigma (pyscf/lib/mcscf GAS library
 with one subspace, built into oracle/_ref) on all host cores.
