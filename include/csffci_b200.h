@@ -211,7 +211,7 @@ enum {
                                       formed, then sigma = s + eta * s^T */
   CSFFCI_SIGMA_REFERENCE_KERNEL = 4, /* force the simple shared-memory-h2e
                                         kernel (used to cross-check) */
-  CSFFCI_SIGMA_DETERMINISTIC = 8 /* bit-identical reruns (8 <= norb <= 16):
+  CSFFCI_SIGMA_DETERMINISTIC = 8 /* bit-identical reruns (4 <= norb <= 16):
                                     every scattered contribution is split
                                     into three fixed-point digits (weights
                                     2^-80, 2^-37, 2^6) added by 64-bit
@@ -269,10 +269,15 @@ void csffci_sigma_plan_destroy(csffci_sigma_plan_t* plan);
 /* One sigma of a batch (csffci_sigma_batch).  The caller fills the first
  * block; the library fills the rest.  sym = 1 asserts neleca == nelecb and
  * ci = eta ci^T (the spin-symmetric kernel) and needs scratch (ndet
- * doubles); otherwise scratch may be NULL.  live (device, may be NULL)
- * gates the job at run time: it runs only when live_index < *live (used by
- * the device-resident batched solver, whose number of new vectors per
- * problem changes from one iteration to the next). */
+ * doubles); otherwise scratch may be NULL.  flags may hold
+ * CSFFCI_SIGMA_JOB_DETERMINISTIC (the scatter of CSFFCI_SIGMA_DETERMINISTIC,
+ * 4 <= norb <= 16; scratch then holds the three int64 digit planes, 3 *
+ * ndet elements, in either mode); all jobs of one call share it.  live
+ * (device, may be NULL) gates the job at run time: it runs only when
+ * live_index < *live (used by the device-resident batched solver, whose
+ * number of new vectors per problem changes from one iteration to the
+ * next). */
+enum { CSFFCI_SIGMA_JOB_DETERMINISTIC = 1 };
 typedef struct {
   const double* h2e;
   const csffci_link_t* link_a;
@@ -282,7 +287,7 @@ typedef struct {
   double* scratch;
   int32_t neleca, nelecb, sym, eta;
   const int32_t* live;
-  int32_t live_index, pad;
+  int32_t live_index, flags;
   /* filled by the library */
   int64_t Na, Nb, unit_begin, nunits, tile_begin, elem_begin;
   int32_t nla, nlb;
@@ -490,7 +495,8 @@ typedef struct {
   int32_t check_every;      /* iterations between completion checks          */
   int32_t use_graph;        /* replay one captured iteration                 */
   int32_t autotune;         /* time the sigma tile variants at bind time     */
-  int32_t pad;
+  int32_t deterministic;    /* sigma with the deterministic scatter (4..16
+                               orbitals): bit-identical reruns            */
 } csffci_batch_options_t;
 
 typedef struct csffci_batch_plan csffci_batch_plan_t;

@@ -19,6 +19,7 @@ SIGMA_ACCUMULATE = 1
 SIGMA_SPIN_SYMMETRIC = 2
 SIGMA_REFERENCE_KERNEL = 4
 SIGMA_DETERMINISTIC = 8
+SIGMA_JOB_DETERMINISTIC = 1
 
 
 class LinkEntry(ctypes.Structure):
@@ -42,7 +43,7 @@ class SigmaJob(ctypes.Structure):
                 ("ci", ctypes.c_void_p), ("sigma", ctypes.c_void_p), ("scratch", ctypes.c_void_p),
                 ("neleca", ctypes.c_int32), ("nelecb", ctypes.c_int32), ("sym", ctypes.c_int32),
                 ("eta", ctypes.c_int32), ("live", ctypes.c_void_p), ("live_index", ctypes.c_int32),
-                ("pad", ctypes.c_int32), ("Na", ctypes.c_int64), ("Nb", ctypes.c_int64),
+                ("flags", ctypes.c_int32), ("Na", ctypes.c_int64), ("Nb", ctypes.c_int64),
                 ("unit_begin", ctypes.c_int64), ("nunits", ctypes.c_int64),
                 ("tile_begin", ctypes.c_int64), ("elem_begin", ctypes.c_int64),
                 ("nla", ctypes.c_int32), ("nlb", ctypes.c_int32)]
@@ -101,7 +102,7 @@ class BatchOptions(ctypes.Structure):
                 ("lindep", ctypes.c_double), ("level_shift", ctypes.c_double),
                 ("max_space", ctypes.c_int32), ("max_cycle", ctypes.c_int32),
                 ("check_every", ctypes.c_int32), ("use_graph", ctypes.c_int32),
-                ("autotune", ctypes.c_int32), ("pad", ctypes.c_int32)]
+                ("autotune", ctypes.c_int32), ("deterministic", ctypes.c_int32)]
 
 
 assert ctypes.sizeof(LinkEntry) == 8

@@ -154,34 +154,40 @@ def _launch_sigma(jobs_by_norb):
         _capi.call("csffci_sigma_batch", norb, len(jobs), arr, ptr(ws), nbytes, stream())
 
 
-def _sigma_job(h2e, la, lb, ci, sigma, scratch, nelec, eta):
+def _sigma_job(h2e, la, lb, ci, sigma, scratch, nelec, eta, deterministic=False):
     j = _capi.SigmaJob()
     j.h2e, j.link_a, j.link_b = h2e.data_ptr(), la.data_ptr(), lb.data_ptr()
     j.ci, j.sigma, j.scratch = ci, sigma, scratch
     j.neleca, j.nelecb = nelec
     j.sym = 1 if eta is not None else 0
     j.eta = eta if eta is not None else 1
+    j.flags = _capi.SIGMA_JOB_DETERMINISTIC if deterministic else 0
     return j
 
 
-def sigma_many(items):
+def sigma_many(items, deterministic=False):
     """sigma = sum h2e[pq,rs] E_pq E_rs ci for many independent problems in
     one launch per orbital count (csffci_sigma_batch).  items: sequence of
     (h2e (npair,npair) device, ci (na*nb) device, norb, (neleca, nelecb),
-    eta or None); eta asserts ci = eta ci^T (neleca == nelecb).  Returns the
-    list of sigma vectors."""
+    eta or None); eta asserts ci = eta ci^T (neleca == nelecb).
+    deterministic: the order-independent scatter (4 <= norb <= 16; each job
+    then takes three int64 digit planes of scratch).  Returns the list of
+    sigma vectors."""
     jobs, outs, keep = {}, [], []
     for h2e, ci, norb, nelec, eta in items:
         nelec = (int(nelec[0]), int(nelec[1]))
         ci = ci.reshape(-1).contiguous()
         out = torch.empty_like(ci)
-        scr = torch.empty_like(ci) if eta is not None else None
+        if deterministic:
+            scr = torch.empty(3 * ci.numel(), dtype=torch.int64, device=ci.device)
+        else:
+            scr = torch.empty_like(ci) if eta is not None else None
         la = D.dev_link_table(norb, nelec[0])
         lb = D.dev_link_table(norb, nelec[1])
         keep += [ci, scr]
         jobs.setdefault(int(norb), []).append(
             _sigma_job(h2e, la, lb, ci.data_ptr(), out.data_ptr(), 0 if scr is None else scr.data_ptr(),
-                       nelec, eta))
+                       nelec, eta, deterministic))
         outs.append(out)
     _launch_sigma(jobs)
     torch.cuda.current_stream().synchronize()
@@ -231,7 +237,7 @@ class BatchedCSFSolver:
 
     def __init__(self, conv_tol=1e-10, lindep=1e-14, max_cycle=100, max_space=12, level_shift=1e-3,
                  pspace_size=200, conv_tol_residual=None, engine="device", check_every=4, use_graph=True,
-                 autotune=True):
+                 autotune=True, deterministic=False):
         self.conv_tol = conv_tol
         self.lindep = lindep
         self.max_cycle = max_cycle
@@ -246,6 +252,10 @@ class BatchedCSFSolver:
         self.check_every = check_every
         self.use_graph = use_graph
         self.autotune = autotune
+        # sigma with the deterministic scatter (4 <= norb <= 16, device
+        # engine): every reduction of the plan then runs in a fixed order and
+        # a rerun gives the same bits
+        self.deterministic = deterministic
         self.iterations = 0
         self.niter = None
         self.tile_variants = None
@@ -349,6 +359,8 @@ class BatchedCSFSolver:
             self._device_davidson(states)
             self._mark("davidson")
         elif self.engine == "host":
+            if self.deterministic:
+                raise ValueError("the deterministic scatter runs with engine='device'")
             self._davidson(states)
         else:
             raise ValueError("engine must be 'device' or 'host'")
@@ -384,7 +396,8 @@ class BatchedCSFSolver:
             q.x0 = x0.data_ptr()
         opt = _capi.BatchOptions(float(self.conv_tol), float(self.conv_tol_residual or 0.0), float(self.lindep),
                                  float(self.level_shift), int(self.max_space), int(self.max_cycle),
-                                 int(self.check_every), 1 if self.use_graph else 0, 1 if self.autotune else 0, 0)
+                                 int(self.check_every), 1 if self.use_graph else 0, 1 if self.autotune else 0,
+                                 1 if self.deterministic else 0)
         plan = ctypes.c_void_p()
         nbytes = ctypes.c_size_t()
         _capi.call("csffci_batch_plan_create", n, probs, ctypes.byref(opt), ctypes.byref(plan), ctypes.byref(nbytes))

@@ -415,9 +415,9 @@ class CSFFCISolver:
     gas_restr = None
     gas_restr_type = _gas.GAS_RESTR_SPIN_SUPERGROUP
     # sigma with the deterministic scatter (CSFFCI_SIGMA_DETERMINISTIC,
-    # 8 <= norb <= 16): reruns give bit-identical sigma vectors, energies
+    # 4 <= norb <= 16): reruns give bit-identical sigma vectors, energies
     # and CI vectors, at the cost of three integer atomics per scattered
-    # element; the solve then takes the host-driven Davidson loop
+    # element (in the host-driven loop and in the device-resident plan)
     deterministic_sigma = False
 
     def __init__(self, mol=None, smult=None):
@@ -532,8 +532,6 @@ class FCISolver(CSFFCISolver, FCIBase):
     def _device_resident_ok(self, h1e, eri, norb, nelec, ci0, kwargs):
         if not self.device_resident or ci0 is not None or not set(kwargs) <= self._DEVICE_KW:
             return False
-        if self.deterministic_sigma:  # the batched plan's sigma uses FP64 atomics
-            return False
         if not isinstance(h1e, np.ndarray) or h1e.ndim != 2 or isinstance(eri, torch.Tensor):
             return False
         if kwargs.get('davidson_only', self.davidson_only):
@@ -553,7 +551,8 @@ class FCISolver(CSFFCISolver, FCIBase):
                                max_space=kwargs.get('max_space', self.max_space), level_shift=self.level_shift,
                                pspace_size=kwargs.get('pspace_size', self.pspace_size),
                                conv_tol_residual=getattr(self, 'conv_tol_residual', None),
-                               autotune=False)  # the defaults are the single-problem shapes
+                               autotune=False,  # the defaults are the single-problem shapes
+                               deterministic=self.deterministic_sigma)
         p = Problem(norb, _unpack_nelec(nelec, self.spin), self.smult, nroots, h1e, eri)
         e, cis, _, conv = sol.kernel([p], with_rdm=False)[0]
         self.phase_s = dict(sol.phase_s)

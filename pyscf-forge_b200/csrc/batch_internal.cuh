@@ -20,6 +20,7 @@ struct SigmaBatchInfo {
   long long total_units = 0, max_nb = 0, nelem = 0, ntiles = 0;
   int max_nla = 0, max_nlb = 0;
   int variant = -1;  // tile shape of the sigma kernel (-1: default for norb)
+  int det = 0;       // the jobs use the deterministic scatter (CSFFCI_SIGMA_JOB_DETERMINISTIC)
   csffci_sigma_job_t job0{};
 };
 int sigma_batch_prepare(int norb, int njobs, csffci_sigma_job_t* jobs, SigmaBatchInfo* info);

@@ -856,6 +856,9 @@ int csffci_batch_plan_create(int nprob, const csffci_batch_problem_t* probs, con
   *plan = nullptr;
   CSF_REQUIRE(nprob > 0 && probs, "batch_plan_create: empty batch");
   CSF_REQUIRE(opt->max_space >= 1 && opt->max_cycle >= 0, "batch_plan_create: bad options");
+  for (int i = 0; i < nprob && opt->deterministic; ++i)
+    CSF_REQUIRE(probs[i].norb >= 4 && probs[i].norb <= 16,
+                "batch_plan_create: the deterministic scatter covers 4 <= norb <= 16, not %d", probs[i].norb);
   auto* P = new csffci_batch_plan();
   P->nprob = nprob;
   P->opt = *opt;
@@ -920,7 +923,11 @@ int csffci_batch_plan_create(int nprob, const csffci_batch_problem_t* probs, con
   for (int i = 0; i < nprob; ++i) {
     const DBProb& d = P->prob[i];
     o_vec[i] = take(sizeof(double) * (size_t)d.n * (2 * d.cap + 6 * d.k));
-    o_det[i] = take(sizeof(double) * (size_t)P->ndet[i] * d.k * (probs[i].eta ? 3 : 2));
+    // det buffers: k vectors, k sigmas, and per root the spin-symmetric
+    // scratch (ndet doubles) or, with the deterministic scatter, the three
+    // int64 digit planes (3 ndet)
+    const int nscr = opt->deterministic ? 3 : (probs[i].eta ? 1 : 0);
+    o_det[i] = take(sizeof(double) * (size_t)P->ndet[i] * d.k * (2 + nscr));
     o_small[i] = take(sizeof(double) * ((size_t)d.cap * d.cap + 3 * (size_t)d.k * d.cap));
   }
   const size_t o_partial = take(sizeof(double) * (size_t)nunits * P->nslot);
@@ -1045,7 +1052,12 @@ int csffci_batch_plan_bind(csffci_batch_plan_t* P, void* arena, size_t arena_byt
         J.link_b = q.link_b;
         J.ci = det + (size_t)v * nd;
         J.sigma = det + (size_t)(q.nroots + v) * nd;
-        J.scratch = q.eta ? det + (size_t)(2 * q.nroots + v) * nd : nullptr;
+        if (P->opt.deterministic) {
+          J.scratch = det + (size_t)(2 * q.nroots + 3 * v) * nd;
+          J.flags = CSFFCI_SIGMA_JOB_DETERMINISTIC;
+        } else {
+          J.scratch = q.eta ? det + (size_t)(2 * q.nroots + v) * nd : nullptr;
+        }
         J.neleca = q.neleca;
         J.nelecb = q.nelecb;
         J.sym = q.eta ? 1 : 0;

@@ -381,7 +381,7 @@ static int sigma_exec(int norb, int neleca, int nelecb, const double* h2e, const
   if (flags & CSFFCI_SIGMA_DETERMINISTIC) {
     CSF_REQUIRE(!(flags & CSFFCI_SIGMA_REFERENCE_KERNEL),
                 "sigma: the deterministic mode runs the warp-specialised kernel, not the reference kernel");
-    CSF_REQUIRE(norb >= 8 && norb <= 16, "sigma: the deterministic mode covers 8 <= norb <= 16, not %d", norb);
+    CSF_REQUIRE(norb >= 4 && norb <= 16, "sigma: the deterministic mode covers 4 <= norb <= 16, not %d", norb);
     const size_t need = csffci_sigma_workspace(norb, neleca, nelecb, flags);
     if (work == nullptr || work_bytes < need) {
       set_error("sigma: workspace of %zu bytes < %zu required", work_bytes, need);
@@ -518,8 +518,8 @@ int csffci_sigma_plan_create(int norb, int neleca, int nelecb, const double* h2e
                          CSFFCI_SIGMA_DETERMINISTIC)) == 0,
               "sigma_plan_create: flags may hold SPIN_SYMMETRIC, REFERENCE_KERNEL and DETERMINISTIC only");
   CSF_REQUIRE(!(flags & CSFFCI_SIGMA_DETERMINISTIC) ||
-                  (norb >= 8 && norb <= 16 && !(flags & CSFFCI_SIGMA_REFERENCE_KERNEL)),
-              "sigma_plan_create: the deterministic mode covers 8 <= norb <= 16 (warp-specialised kernel)");
+                  (norb >= 4 && norb <= 16 && !(flags & CSFFCI_SIGMA_REFERENCE_KERNEL)),
+              "sigma_plan_create: the deterministic mode covers 4 <= norb <= 16 (warp-specialised kernel)");
   CSF_REQUIRE(!(flags & CSFFCI_SIGMA_SPIN_SYMMETRIC) || neleca == nelecb,
               "sigma_plan_create: the spin-symmetric mode needs neleca == nelecb");
   csffci_sigma_plan_t* p = new (std::nothrow) csffci_sigma_plan_t;

@@ -220,7 +220,72 @@ __global__ void k_batch_zero(const csffci_sigma_job_t* jobs, int njobs, long lon
     while (j + 1 < njobs && jobs[j + 1].elem_begin <= i) ++j;
     const csffci_sigma_job_t& J = jobs[j];
     if (!job_live(J)) continue;
-    (J.sym ? J.scratch : J.sigma)[i - J.elem_begin] = 0.0;
+    const long long li = i - J.elem_begin;
+    if (J.flags & CSFFCI_SIGMA_JOB_DETERMINISTIC) {  // the three digit planes
+      long long* w = reinterpret_cast<long long*>(J.scratch);
+      const long long nd = J.Na * J.Nb;
+      w[li] = w[nd + li] = w[2 * nd + li] = 0;
+    } else {
+      (J.sym ? J.scratch : J.sigma)[li] = 0.0;
+    }
+  }
+}
+
+// the digit planes of a deterministic job -> sigma (k_det_finish's value;
+// general jobs elementwise here, spin-symmetric ones by k_batch_det_sym)
+__device__ __forceinline__ double batch_det_value(long long w0, long long w1, long long w2) {
+  return ((double)w2 * 0x1p6 + (double)w1 * 0x1p-37) + (double)w0 * 0x1p-80;
+}
+
+__global__ void k_batch_det_finish(const csffci_sigma_job_t* jobs, int njobs, long long total) {
+  int j = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    while (j + 1 < njobs && jobs[j + 1].elem_begin <= i) ++j;
+    const csffci_sigma_job_t& J = jobs[j];
+    if (J.sym || !job_live(J)) continue;
+    const long long li = i - J.elem_begin, nd = J.Na * J.Nb;
+    const long long* w = reinterpret_cast<const long long*>(J.scratch);
+    J.sigma[li] = batch_det_value(w[li], w[nd + li], w[2 * nd + li]);
+  }
+}
+
+// sigma = S + eta S^T of spin-symmetric deterministic jobs, the digit words
+// of the two entries added as integers before the conversion
+__global__ void k_batch_det_sym(const csffci_sigma_job_t* jobs, int njobs, long long total_tiles) {
+  __shared__ long long tile[3][32][33];
+  int j = 0;
+  for (long long t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+    while (j + 1 < njobs && jobs[j + 1].tile_begin <= t) ++j;
+    while (!jobs[j].sym) ++j;  // general jobs own no tiles
+    const csffci_sigma_job_t& J = jobs[j];
+    if (!job_live(J)) continue;  // uniform over the block (one tile per block)
+    const long long n = J.Na, nd = n * n;
+    const long long ntile = (n + 31) / 32;
+    const long long lt = t - J.tile_begin;
+    const long long ti = lt / ntile, tj = lt - ti * ntile;
+    const long long* w = reinterpret_cast<const long long*>(J.scratch);
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const long long row = tj * 32 + r, col = ti * 32 + threadIdx.x;
+      const bool in = row < n && col < n;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) tile[k][r][threadIdx.x] = in ? w[k * nd + row * n + col] : 0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const long long row = ti * 32 + r, col = tj * 32 + threadIdx.x;
+      if (row < n && col < n) {
+        long long d[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const unsigned long long a = (unsigned long long)w[k * nd + row * n + col];
+          const unsigned long long b = (unsigned long long)tile[k][threadIdx.x][r];
+          d[k] = (long long)(J.eta > 0 ? a + b : a - b);
+        }
+        J.sigma[row * n + col] = batch_det_value(d[0], d[1], d[2]);
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -267,6 +332,12 @@ int sigma_batch_prepare(int norb, int njobs, csffci_sigma_job_t* jobs, SigmaBatc
     CSF_REQUIRE(rr_aligned8(J.link_a) && rr_aligned8(J.link_b) && rr_aligned8(J.ci) && rr_aligned8(J.sigma) &&
                     rr_aligned8(J.scratch),
                 "sigma_batch: job %d has a pointer that is not 8-byte aligned", i);
+    CSF_REQUIRE((J.flags & ~CSFFCI_SIGMA_JOB_DETERMINISTIC) == 0 &&
+                    (J.flags & CSFFCI_SIGMA_JOB_DETERMINISTIC) == (jobs[0].flags & CSFFCI_SIGMA_JOB_DETERMINISTIC),
+                "sigma_batch: job %d: flags must be 0 or DETERMINISTIC, the same for every job", i);
+    CSF_REQUIRE(!(J.flags & CSFFCI_SIGMA_JOB_DETERMINISTIC) || (J.scratch != nullptr && sigma_ws_supported(norb)),
+                "sigma_batch: job %d: the deterministic scatter needs scratch (3*ndet int64) and 4 <= norb <= 16",
+                i);
   }
   info->norb = norb;
   info->njobs = njobs;
@@ -276,6 +347,8 @@ int sigma_batch_prepare(int norb, int njobs, csffci_sigma_job_t* jobs, SigmaBatc
   for (int i = 0; i < njobs; ++i)
     if (jobs[i].sym) info->ntiles = jobs[i].tile_begin + ((jobs[i].Na + 31) / 32) * ((jobs[i].Na + 31) / 32);
   info->job0 = jobs[0];
+  info->det = (jobs[0].flags & CSFFCI_SIGMA_JOB_DETERMINISTIC) ? 1 : 0;
+  if (info->det) info->variant = RR_VARIANT_WS;  // the only kernel with the deterministic scatter
   return CSFFCI_OK;
 }
 
@@ -288,6 +361,23 @@ int sigma_batch_launch(const SigmaBatchInfo& info, const csffci_sigma_job_t* dj,
   // a gated single job goes through the job-table kernel (the by-value
   // form cannot see the gate)
   const bool table = njobs > 1 || info.job0.live != nullptr;
+  if (info.det) {
+    // the job table's form of the deterministic kernel (each job's planes
+    // are its own Na*Nb apart), then sigma from the planes
+    st = sigma_rr_launch(info.norb, njobs, dj, info.job0, info.total_units, info.max_nb, info.max_nla,
+                         info.max_nlb, stream, RR_VARIANT_WS, 1);
+    if (st) return st;
+    {
+      ProfScope ps("k_batch_det_finish", stream);
+      k_batch_det_finish<<<grid_for(info.nelem, 256, 148 * 16), 256, 0, stream>>>(dj, njobs, info.nelem);
+    }
+    st = check_launch("sigma_batch deterministic finish");
+    if (st || info.ntiles == 0) return st;
+    dim3 blk(32, 8);
+    ProfScope ps("k_batch_det_sym", stream);
+    k_batch_det_sym<<<grid_for(info.ntiles, 1, 148 * 16), blk, 0, stream>>>(dj, njobs, info.ntiles);
+    return check_launch("sigma_batch deterministic symmetric finish");
+  }
   st = table ? sigma_rr_launch(info.norb, njobs, dj, info.job0, info.total_units, info.max_nb,
                                info.max_nla, info.max_nlb, stream, info.variant)
              : sigma_rr_launch(info.norb, 1, nullptr, info.job0, info.total_units, info.max_nb,
@@ -322,6 +412,7 @@ static unsigned long long job_signature(const csffci_sigma_job_t* jobs, int njob
 
 int sigma_batch_tune(SigmaBatchInfo& info, const csffci_sigma_job_t* jobs_host, const csffci_sigma_job_t* dj,
                      cudaStream_t stream) {
+  if (info.det) return CSFFCI_OK;  // one kernel has the deterministic scatter: nothing to choose
   const auto key = std::make_pair(info.norb, job_signature(jobs_host, info.njobs));
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);

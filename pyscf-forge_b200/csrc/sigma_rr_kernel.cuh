@@ -447,7 +447,7 @@ static int launch_rr(RRArgs& g, size_t smem, cudaStream_t stream) {
 
 // tile-shape variants: (rows per warp, n-tiles of 8 columns)
 constexpr int RR_NVARIANT = 4;
-// the warp-specialised kernel (sigma_ws.cu), 8..16 orbitals, one problem
+// the warp-specialised kernel (sigma_ws.cu), 4..16 orbitals, one problem
 // or a job table: one MMA warp per 8 rows (variant 4) or, up to 12
 // orbitals, per 16 rows in CTAs of 8 warps (variant 7)
 constexpr int RR_VARIANT_WS = 4;

@@ -1,10 +1,11 @@
-// Warp-specialised variant of the register-resident sigma kernel, 8..16
+// Warp-specialised variant of the register-resident sigma kernel, 4..16
 // orbitals: tile variant 4 (one MMA warp per 8 rows) and, up to 12 orbitals,
 // variant 7 (one MMA warp per 16 rows, m16n8k4, in CTAs of 8 warps).  Either
 // runs one problem or a job table of many (BATCH: each unit's job is looked
 // up between two barrier-9 syncs, gated jobs are skipped by both roles); the
-// one-problem form with 8-row warps also has the deterministic scatter (DET:
-// integer digit planes instead of FP64 atomics, det_add3).
+// form with 8-row warps also has the deterministic scatter (DET: integer
+// digit planes instead of FP64 atomics, det_add3), for one problem or a job
+// table.
 //
 // k_sigma_rr runs the gather, MMA and scatter phases of a tile one after the
 // other, separated by block barriers, so the FP64 tensor pipe idles while
@@ -234,15 +235,16 @@ __global__ void __launch_bounds__(WSLayout<MT, MW>::NTOT * 32, MINB) k_sigma_ws(
           // of it stays in registers across the MMA
           const long long aoff = r0 < npair ? S.apoff[r0] : -1;
           if (aoff >= 0) {
-            double* const abase = (sjob.sym ? sjob.scratch : sjob.sigma) + aoff;
+            double* const abase = ((sjob.sym || DET) ? sjob.scratch : sjob.sigma) + aoff;
+            const long long dstr = BATCH ? sjob.Na * sjob.Nb : g.det_stride;
             const unsigned aneg = S.pneg[srow.pc + r0];
             const int alim = (int)(sjob.sym ? srow.ja : sjob.Nb);
             const int J = (srow.c0 + c) * NB + 8 * t0 + 2 * tq;
-            if (J < alim) ws_out_add<DET>(abase + J, rr_flip(acc[0][0], aneg), g.det_stride);
-            if (J + 1 < alim) ws_out_add<DET>(abase + J + 1, rr_flip(acc[0][1], aneg), g.det_stride);
+            if (J < alim) ws_out_add<DET>(abase + J, rr_flip(acc[0][0], aneg), dstr);
+            if (J + 1 < alim) ws_out_add<DET>(abase + J + 1, rr_flip(acc[0][1], aneg), dstr);
             if (!part) {
-              if (J + 8 < alim) ws_out_add<DET>(abase + J + 8, rr_flip(acc[1][0], aneg), g.det_stride);
-              if (J + 9 < alim) ws_out_add<DET>(abase + J + 9, rr_flip(acc[1][1], aneg), g.det_stride);
+              if (J + 8 < alim) ws_out_add<DET>(abase + J + 8, rr_flip(acc[1][0], aneg), dstr);
+              if (J + 9 < alim) ws_out_add<DET>(abase + J + 9, rr_flip(acc[1][1], aneg), dstr);
             }
           }
         }
@@ -253,7 +255,7 @@ __global__ void __launch_bounds__(WSLayout<MT, MW>::NTOT * 32, MINB) k_sigma_ws(
   }
 }
 
-bool sigma_ws_supported(int norb) { return norb >= 8 && norb <= 16; }
+bool sigma_ws_supported(int norb) { return norb >= 4 && norb <= 16; }
 bool sigma_ws16_supported(int norb) { return norb >= 8 && norb <= 12; }
 
 // CTAs per SM the registers are sized for: below 13 orbitals the A
@@ -267,9 +269,10 @@ static int launch_ws(RRArgs& g, size_t smem, cudaStream_t stream) {
   // 16-row MMA warps: 8-warp CTAs, two per SM
   constexpr int MINB = MW == 16 ? 2 : ws_min_blocks(NORB);
   // the deterministic scatter: one problem, 8-row MMA warps only
-  auto kern = g.jobs ? k_sigma_ws<KS, MT, MW, true, MINB>
-              : (MW == 8 && g.det_stride) ? k_sigma_ws<KS, MT, MW, false, MINB, MW == 8>
-                                          : k_sigma_ws<KS, MT, MW, false, MINB>;
+  auto kern = g.jobs ? ((MW == 8 && g.det_stride) ? k_sigma_ws<KS, MT, MW, true, MINB, MW == 8>
+                                                  : k_sigma_ws<KS, MT, MW, true, MINB>)
+                     : ((MW == 8 && g.det_stride) ? k_sigma_ws<KS, MT, MW, false, MINB, MW == 8>
+                                                  : k_sigma_ws<KS, MT, MW, false, MINB>);
   CSF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, nsm = 148, per_sm = 0;
   CSF_CUDA(cudaGetDevice(&dev));
@@ -283,7 +286,8 @@ static int launch_ws(RRArgs& g, size_t smem, cudaStream_t stream) {
   ws_split_last_round(g, grid);
   if (grid > g.total_units) grid = g.total_units;
   if (grid < 1) return CSFFCI_OK;
-  static const char* names8[17] = {"", "", "", "", "", "", "", "", "k_sigma_ws_n8", "k_sigma_ws_n9",
+  static const char* names8[17] = {"", "", "", "", "k_sigma_ws_n4", "k_sigma_ws_n5", "k_sigma_ws_n6",
+                                   "k_sigma_ws_n7", "k_sigma_ws_n8", "k_sigma_ws_n9",
                                    "k_sigma_ws_n10", "k_sigma_ws_n11", "k_sigma_ws_n12", "k_sigma_ws_n13",
                                    "k_sigma_ws_n14", "k_sigma_ws_n15", "k_sigma_ws_n16"};
   static const char* names16[13] = {"", "", "", "", "", "", "", "", "k_sigma_ws16_n8", "k_sigma_ws16_n9",
@@ -332,8 +336,8 @@ int sigma_ws_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev, con
     set_error("sigma: no warp-specialised kernel with %d-row MMA warps for norb %d", mw, norb);
     return CSFFCI_ERR_INVALID;
   }
-  if (det_stride && (jobs_dev || mw != 8)) {
-    set_error("sigma: the deterministic scatter takes one problem and 8-row MMA warps");
+  if (det_stride && mw != 8) {
+    set_error("sigma: the deterministic scatter runs with 8-row MMA warps");
     return CSFFCI_ERR_INVALID;
   }
   const int npair = norb * (norb + 1) / 2;
@@ -361,6 +365,10 @@ int sigma_ws_launch(int norb, int njobs, const csffci_sigma_job_t* jobs_dev, con
     }
   }
   switch (norb) {  // KS = ceil(npair / 4), MT = ceil(npair / 8)
+    case 4: return launch_ws<3, 2, 4, 8>(g, smem, stream);
+    case 5: return launch_ws<4, 2, 5, 8>(g, smem, stream);
+    case 6: return launch_ws<6, 3, 6, 8>(g, smem, stream);
+    case 7: return launch_ws<7, 4, 7, 8>(g, smem, stream);
     case 8: return launch_ws<9, 5, 8, 8>(g, smem, stream);
     case 9: return launch_ws<12, 6, 9, 8>(g, smem, stream);
     case 10: return launch_ws<14, 7, 10, 8>(g, smem, stream);

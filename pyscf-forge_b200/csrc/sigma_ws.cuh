@@ -238,7 +238,10 @@ __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S
       const int nla = sjob.nla, nlb = sjob.nlb, nz = srow.nzero;
       const unsigned* pc = S.pneg + srow.pc;
       const bool SYM = sjob.sym != 0;
-      double* const out = SYM ? sjob.scratch : sjob.sigma;
+      // the deterministic scatter writes the digit planes in scratch, whose
+      // planes are Na*Nb apart (a job table's) or g.det_stride (one problem)
+      double* const out = (SYM || DET) ? sjob.scratch : sjob.sigma;
+      const long long dstr = BATCH ? sjob.Na * sjob.Nb : g.det_stride;
       for (int c = 0; c <= nch + 1; ++c) {
         // every mover has finished step c-1 (its scatter read the stage
         // that the copies below refill)
@@ -357,7 +360,7 @@ __device__ __forceinline__ void ws_mover_role(const RRArgs& g, const WSShared& S
               for (int k = 0; k < RU; ++k) v[k] = D[rr_lpair(e[k]) * ds + jl];
 #pragma unroll
               for (int k = 0; k < RU; ++k)
-                if (m0 + k * MPASS < nlb) ws_out_add<DET>(&orow[e[k].x], rr_flip(v[k], rr_lneg(e[k])), g.det_stride);
+                if (m0 + k * MPASS < nlb) ws_out_add<DET>(&orow[e[k].x], rr_flip(v[k], rr_lneg(e[k])), dstr);
             }
           }
         }

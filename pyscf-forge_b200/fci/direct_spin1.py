@@ -96,7 +96,7 @@ class SigmaPlan:
     Holds references to h2e and the link tables, whose device memory the
     plan borrows; the kernel is fixed at creation (CSFFCI_SIGMA_VARIANT is
     read then).  deterministic: the scatter of CSFFCI_SIGMA_DETERMINISTIC
-    (bit-identical reruns, 8 <= norb <= 16)."""
+    (bit-identical reruns, 4 <= norb <= 16)."""
 
     def __init__(self, h2e, norb, nelec, spin_symmetric=False, deterministic=False):
         require_cuda()

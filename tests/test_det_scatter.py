@@ -89,7 +89,7 @@ def test_symmetric_finish_adds_digits_first():
 
 def test_plan_flag_checks():
     """csffci_sigma_plan_create with CSFFCI_SIGMA_DETERMINISTIC: the digit
-    planes as workspace and the warp-specialised kernel inside 8..16
+    planes as workspace and the warp-specialised kernel inside 4..16
     orbitals; refused outside it and with the reference kernel.  create
     only records the borrowed pointers, so placeholders do here."""
     from math import comb
@@ -97,7 +97,8 @@ def test_plan_flag_checks():
     lib = _capi.load()
     dummy = ctypes.c_void_p(16)
     det = _capi.SIGMA_DETERMINISTIC
-    for norb, nelec, extra in ((12, (6, 6), _capi.SIGMA_SPIN_SYMMETRIC), (10, (5, 4), 0), (16, (3, 2), 0)):
+    for norb, nelec, extra in ((12, (6, 6), _capi.SIGMA_SPIN_SYMMETRIC), (10, (5, 4), 0), (16, (3, 2), 0),
+                               (4, (2, 1), 0)):
         h = ctypes.c_void_p()
         nbytes = ctypes.c_size_t()
         st = lib.csffci_sigma_plan_create(norb, nelec[0], nelec[1], dummy, dummy, dummy, det | extra,
@@ -107,7 +108,7 @@ def test_plan_flag_checks():
         assert lib.csffci_sigma_plan_variant(h) == 4
         lib.csffci_sigma_plan_destroy(h)
         assert lib.csffci_sigma_workspace(norb, nelec[0], nelec[1], det) == nbytes.value
-    for norb, flags in ((6, det), (17, det), (12, det | _capi.SIGMA_REFERENCE_KERNEL)):
+    for norb, flags in ((3, det), (17, det), (12, det | _capi.SIGMA_REFERENCE_KERNEL)):
         h = ctypes.c_void_p()
         st = lib.csffci_sigma_plan_create(norb, 3, 3, dummy, dummy, dummy, flags, ctypes.byref(h), None)
         assert st == _capi.CSFFCI_ERR_INVALID

@@ -53,7 +53,7 @@ def test_sigma_many_matches_single_and_oracle():
 @pytest.mark.parametrize("variant", ["4", "7"])
 def test_sigma_many_warp_specialised_job_table(monkeypatch, variant):
     """The warp-specialised kernel over a job table: variant 4 (8-row MMA
-    warps, 8..16 orbitals; the default at 10..12 and 14..16) and variant 7
+    warps, 4..16 orbitals; the default at 10..12 and 14..16) and variant 7
     (16-row MMA warps in 8-warp CTAs, 8..12 orbitals), both autotuner
     candidates.  Jobs past a variant's orbital range run the default kernel:
     jobs of mixed electron counts and symmetric / general / antisymmetric

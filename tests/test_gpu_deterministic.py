@@ -3,7 +3,7 @@ scattered contribution goes into three int64 digit planes by integer
 atomics, so a rerun gives the same bits whatever order the atomics land
 in.  Checked: two runs are bit-identical (torch.equal) in the general,
 spin-symmetric (eta = +1) and antisymmetric (eta = -1) modes and with
-accumulation, at CAS(10,10) up to the benchmarked CAS(16,16) (8,8); the
+accumulation, from 4 orbitals up to the benchmarked CAS(16,16) (8,8); the
 result agrees with the FP64-atomic kernel to 1e-12 and with the
 reference's own CPU sigma (fci_contract_gas_plan_execute,
 pyscf/lib/mcscf/fci_contract_gas.c:2423-2452) to the 1e-9 sigma bar; a
@@ -37,7 +37,8 @@ def _case(norb, nelec, eta, seed):
 
 @pytest.mark.parametrize("norb,nelec,eta", [(10, (5, 5), None), (10, (5, 5), 1), (10, (5, 5), -1),
                                             (12, (6, 5), None), (12, (6, 6), 1), (14, (7, 7), -1),
-                                            (8, (4, 3), None)])
+                                            (8, (4, 3), None), (6, (3, 3), 1), (4, (2, 1), None),
+                                            (7, (4, 3), None)])
 def test_deterministic_sigma_repeats_and_matches(norb, nelec, eta):
     from pyscf_forge_b200.fci import direct_spin1 as D
     h2e_np, c = _case(norb, nelec, eta, seed=norb * 13 + nelec[1])
@@ -89,9 +90,11 @@ def test_deterministic_sigma_cas16():
     assert float((a - ref).abs().max()) < SIGMA_ATOL
 
 
-def test_deterministic_solve_repeats():
-    """FCISolver with deterministic_sigma (the host-driven Davidson loop,
-    every reduction in a fixed order): two solves of CAS(10,10) with three
+@pytest.mark.parametrize("device_resident", [False, True])
+def test_deterministic_solve_repeats(device_resident):
+    """FCISolver with deterministic_sigma, in the host-driven Davidson loop
+    and in the device-resident plan (every reduction in a fixed order in
+    both): two solves of CAS(10,10) with three
     singlet roots give the same energies and CI vectors bit for bit, and
     energies within 1e-9 Eh of the default solver and of the exact singlet
     roots (scipy eigsh over the reference's sigma, S^2 from the oracle:
@@ -110,6 +113,7 @@ def test_deterministic_solve_repeats():
         sol.max_space = 30
         sol.max_cycle = 400
         sol.deterministic_sigma = det
+        sol.device_resident = device_resident
         e, ci = sol.kernel(h1, eri, 10, (5, 5))
         assert np.all(sol.converged)
         res.append((np.asarray(e), [np.asarray(x) for x in ci]))
@@ -118,3 +122,48 @@ def test_deterministic_solve_repeats():
     assert all(np.array_equal(x, y) for x, y in zip(c1, c2))
     np.testing.assert_allclose(e1, e3, atol=1e-9)
     np.testing.assert_allclose(e1, [-17.31158032, -17.19811638, -16.82364217], atol=1e-7)
+
+
+def test_deterministic_sigma_many():
+    """The job-table form (csffci_sigma_batch with every job flagged
+    CSFFCI_SIGMA_JOB_DETERMINISTIC): mixed orbital counts 4..16, general,
+    symmetric and antisymmetric jobs in one call; two calls bit-identical,
+    each job against the one-problem deterministic sigma (bit-identical:
+    the same digit sums) and the reference sigma."""
+    from pyscf_forge_b200 import batched as B
+    from pyscf_forge_b200.fci import direct_spin1 as D
+    cases = [(4, (2, 1), None), (6, (3, 3), 1), (8, (4, 4), -1), (8, (4, 3), None), (10, (5, 5), 1),
+             (12, (6, 5), None), (12, (2, 2), -1), (16, (3, 2), None)]
+    items, host = [], []
+    for i, (norb, nelec, eta) in enumerate(cases):
+        h2e_np, c = _case(norb, nelec, eta, seed=40 + i)
+        items.append((torch.as_tensor(h2e_np, device="cuda"), torch.as_tensor(c.ravel(), device="cuda"),
+                      norb, nelec, eta))
+        host.append((h2e_np, c))
+    a = B.sigma_many(items, deterministic=True)
+    b = B.sigma_many(items, deterministic=True)
+    for (h2e, cd, norb, nelec, eta), x, y, (h2e_np, c) in zip(items, a, b, host):
+        assert torch.equal(x, y), (norb, nelec, eta)
+        one = D.dev_contract_2e(h2e, cd, norb, nelec, eta=eta, deterministic=True)
+        assert torch.equal(x, one), (norb, nelec, eta)
+        if gasref.available():
+            ref = gasref.contract_2e(h2e_np, c, norb, nelec).ravel()
+            assert float(np.abs(x.cpu().numpy() - ref).max()) < SIGMA_ATOL
+
+
+def test_deterministic_batched_solver_repeats():
+    """BatchedCSFSolver(deterministic=True): an uneven batch (norb 6..10,
+    1-4 roots, several spins) solved twice gives the same energies and CI
+    vectors bit for bit, and energies within 1e-10 Eh of the default
+    batched solver."""
+    from pyscf_forge_b200 import batched as B
+    probs = B.make_uneven_batch(10, seed0=5000, norb_lo=6, norb_hi=10)
+    kw = dict(conv_tol=1e-12, conv_tol_residual=1e-7, max_cycle=400, max_space=30)
+    r1 = B.BatchedCSFSolver(deterministic=True, **kw).kernel(probs, with_rdm=False)
+    r2 = B.BatchedCSFSolver(deterministic=True, **kw).kernel(probs, with_rdm=False)
+    r3 = B.BatchedCSFSolver(**kw).kernel(probs, with_rdm=False)
+    for p, x, y, z in zip(probs, r1, r2, r3):
+        assert x[3] and y[3] and z[3]
+        assert np.array_equal(np.asarray(x[0]), np.asarray(y[0])), (p.norb, p.nelec, p.smult)
+        assert all(np.array_equal(np.asarray(u), np.asarray(v)) for u, v in zip(x[1], y[1]))
+        np.testing.assert_allclose(x[0], z[0], atol=1e-10)
