@@ -58,10 +58,12 @@ struct DBProb {
   double *V, *AV, *X, *AX, *R, *T, *W, *AW;
   const double* hdiag;
   double *h, *coef, *cc, *xprev;
+  double *qprev, *dprev;  // eigenvectors (cap x cap) and eigenvalues of the last subspace matrix
 };
 
 struct DBState {
-  int32_t m, m_old, kT, knew, kk, done, restart, niter, any_conv, have_e, kk_prev, pad;
+  int32_t m, m_old, kT, knew, kk, done, restart, niter, any_conv, have_e, kk_prev;
+  int32_t mq;  // size of the basis qprev/dprev diagonalise (0: none)
   int32_t todo[DB_KMAX];
   int32_t conv[DB_KMAX];
   double e[DB_KMAX], e_prev[DB_KMAX], rnorm[DB_KMAX], e1[DB_KMAX], es[DB_KMAX], tnorm[DB_KMAX];
@@ -407,9 +409,10 @@ __device__ double db_reduce_slot(const DBArgs& a, const DBProb& P, int s) {
 // sections 8.5.2 and 8.5.5).  On return diag(A) holds the eigenvalues and
 // the columns of Q the eigenvectors; w/perm give them in ascending order.
 __device__ void db_jacobi(double* A, double* Q, int n, int ld, double* rot, double* w, int* perm,
-                          double* redbuf) {
+                          double* redbuf, bool qinit = false) {
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int i = tid; i < n * ld; i += nt) Q[i] = ((i / ld) == (i % ld)) ? 1.0 : 0.0;
+  if (!qinit)  // else Q holds a starting basis the rotations are applied to
+    for (int i = tid; i < n * ld; i += nt) Q[i] = ((i / ld) == (i % ld)) ? 1.0 : 0.0;
   const int nn = n + (n & 1);
   const int np = nn / 2;
   __syncthreads();
@@ -604,12 +607,38 @@ __global__ void __launch_bounds__(DB_ST) k_db_sritz(DBArgs a) {
     }
   }
   __syncthreads();
+  // Warm start: the first m0 basis vectors were diagonalised at the last
+  // iteration (eigenvectors qprev, eigenvalues dprev; after a restart the
+  // identity and the Ritz values).  In the basis diag(qprev, I) the matrix
+  // is diag(dprev) bordered by the new rows and columns, which the Jacobi
+  // sweeps then clear in a few sweeps instead of diagonalising from scratch
+  // (the off-diagonal entries dropped there are below the Jacobi tolerance
+  // of the last solve).  Both border halves sum in the same order, so A
+  // stays exactly symmetric.
+  const bool warm = S.mq == m0 && m0 > 0;
   for (int idx = tid; idx < m * m; idx += DB_ST) {
     const int i = idx / m, j = idx % m;
-    A[i * ld + j] = P.h[i * cap + j];
+    double v;
+    if (!warm || (i >= m0 && j >= m0)) {
+      v = P.h[i * cap + j];
+    } else if (i < m0 && j < m0) {
+      v = i == j ? P.dprev[i] : 0.0;
+    } else {
+      const int r = i < m0 ? i : j, c = i < m0 ? j : i;  // qprev column r, new column c
+      v = 0.0;
+      for (int l = 0; l < m0; ++l) v = fma(P.qprev[l * cap + r], P.h[l * cap + c], v);
+    }
+    A[i * ld + j] = v;
+    if (warm) Q[i * ld + j] = (i < m0 && j < m0) ? P.qprev[i * cap + j] : (i == j ? 1.0 : 0.0);
   }
   __syncthreads();
-  db_jacobi(A, Q, m, ld, rot, w, perm, redbuf);
+  db_jacobi(A, Q, m, ld, rot, w, perm, redbuf, warm);
+  // the eigenpairs of this basis, for the next iteration's warm start
+  for (int idx = tid; idx < m * m; idx += DB_ST) {
+    const int i = idx / m, j = idx % m;
+    P.qprev[i * cap + j] = Q[i * ld + j];
+  }
+  for (int i = tid; i < m; i += DB_ST) P.dprev[i] = A[i * ld + i];
   const int kk = m < P.k ? m : P.k;
   const bool follow = S.have_e && S.any_conv;
   if (follow) {
@@ -713,6 +742,7 @@ __global__ void __launch_bounds__(DB_ST) k_db_sconv(DBArgs a) {
     S.knew = 0;  // set again by the next orthonormalisation
     S.restart = !S.done && (S.m + kT > P.space);
     if (S.restart) S.m = kk;
+    S.mq = S.restart ? kk : S.m;  // the basis the stored eigenpairs belong to
     restart_s = S.restart;
     done_s = S.done;
   }
@@ -726,11 +756,15 @@ __global__ void __launch_bounds__(DB_ST) k_db_sconv(DBArgs a) {
     const int i = idx / cap, j = idx % cap;
     P.xprev[idx] = restart ? (i == j ? 1.0 : 0.0) : P.cc[idx];
   }
-  if (restart)
+  if (restart) {
+    // the basis is the Ritz vectors: h = diag(e), eigenvectors the identity
     for (int idx = tid; idx < cap * cap; idx += DB_ST) {
       const int i = idx / cap, j = idx % cap;
       P.h[idx] = (i == j && i < kk) ? S.e[i] : 0.0;
+      P.qprev[idx] = (i == j && i < kk) ? 1.0 : 0.0;
     }
+    for (int i = tid; i < kk; i += DB_ST) P.dprev[i] = S.e[i];
+  }
 }
 
 __global__ void k_db_init(DBArgs a, const double* const* x0) {
@@ -928,7 +962,7 @@ int csffci_batch_plan_create(int nprob, const csffci_batch_problem_t* probs, con
     // int64 digit planes (3 ndet)
     const int nscr = opt->deterministic ? 3 : (probs[i].eta ? 1 : 0);
     o_det[i] = take(sizeof(double) * (size_t)P->ndet[i] * d.k * (2 + nscr));
-    o_small[i] = take(sizeof(double) * ((size_t)d.cap * d.cap + 3 * (size_t)d.k * d.cap));
+    o_small[i] = take(sizeof(double) * (2 * (size_t)d.cap * d.cap + 3 * (size_t)d.k * d.cap + d.cap));
   }
   const size_t o_partial = take(sizeof(double) * (size_t)nunits * P->nslot);
   const size_t o_prob = take(sizeof(DBProb) * nprob);
@@ -1010,6 +1044,8 @@ int csffci_batch_plan_bind(csffci_batch_plan_t* P, void* arena, size_t arena_byt
     d.coef = sm + (size_t)d.cap * d.cap;
     d.cc = d.coef + (size_t)d.k * d.cap;
     d.xprev = d.cc + (size_t)d.k * d.cap;
+    d.qprev = d.xprev + (size_t)d.k * d.cap;
+    d.dprev = d.qprev + (size_t)d.cap * d.cap;
   }
   P->args.partial = (double*)rel(P->args.partial);
   P->args.prob = (const DBProb*)rel(P->args.prob);
